@@ -1,0 +1,140 @@
+/*
+ * pfb200.h -- C ABI of the B200 Pfaffian engine (libpfb200.so).
+ *
+ * Plain C types only: device pointers, sizes, enums and a cudaStream_t passed as
+ * void*.  Every entry point
+ *   - enqueues its work on `stream` and returns without synchronising the host,
+ *   - allocates nothing: scratch memory is the caller's `workspace`, whose size
+ *     the matching *_workspace_bytes function gives,
+ *   - never throws and never writes its input; errors come back as a pfb_status,
+ *   - is re-entrant (no global mutable state), so several streams or threads may
+ *     call it at once.
+ *
+ * Matrices are batches of `batch` contiguous n x n arrays.  `layout` says how one
+ * matrix is stored: PFB_ROW_MAJOR (C order, torch/NumPy default) or PFB_COL_MAJOR
+ * (how XLA hands a matrix to the reference's handlers, which request
+ * input_layouts=[(1, 0)] at pfcuda/cuda_api.py:57,79 and index CM(A,n,r,c) =
+ * A[r + c*n], include/pfaffian_utils.cuh:10).  The inputs are taken to be
+ * skew-symmetric; the Pfaffian of the matrix in the stated layout is returned.
+ *
+ * Complex values are interleaved (re, im) pairs of float (C64) or double (C128).
+ */
+#ifndef PFB200_H
+#define PFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PFB_F32 = 0,   /* float            */
+    PFB_F64 = 1,   /* double           */
+    PFB_C64 = 2,   /* complex float    */
+    PFB_C128 = 3   /* complex double   */
+} pfb_dtype;
+
+typedef enum {
+    PFB_ROW_MAJOR = 0,
+    PFB_COL_MAJOR = 1
+} pfb_layout;
+
+/* Arithmetic of the trailing skew rank-2k update of the blocked factorisation.
+ * The panel (pivot search, interchanges, Gauss vectors, log|Pf| and sign) is
+ * always FP64 (complex128 for complex input). */
+typedef enum {
+    PFB_MODE_FP64 = 0,   /* FP64 / complex128 update                                */
+    PFB_MODE_SPLIT = 1   /* error-free int8 slices on the tcgen05 tensor cores with
+                            exact int32 accumulation, recombined in FP64             */
+} pfb_mode;
+
+typedef enum {
+    PFB_OK = 0,
+    PFB_ERR_INVALID = 1,     /* null pointer, bad enum, negative batch        */
+    PFB_ERR_SIZE = 2,        /* matrix order outside the entry point's range  */
+    PFB_ERR_WORKSPACE = 3,   /* workspace missing, too small or misaligned    */
+    PFB_ERR_CUDA = 4,        /* a CUDA runtime call failed                    */
+    PFB_ERR_UNSUPPORTED = 5, /* combination not built (e.g. no sm_100a device) */
+    PFB_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up            */
+} pfb_status;
+
+/* Text for a status code (static storage). */
+const char *pfb_status_string(int status);
+
+/* Last CUDA error seen by the calling thread's most recent failing call. */
+int pfb_last_cuda_error(void);
+
+/*
+ * Pf(A) for n <= 32, one value per matrix, in the input dtype.
+ *
+ * Replaces the XLA handlers pfaffian_f32 / _f64 / _c64 / _c128
+ * (bindings/jax_bindings.cu:82-112, symbols :196-228), which launch the
+ * reference kernel pf_sm_calc once per matrix (src/pfaffian_sm.cu:101-105).
+ * Here one launch covers the whole batch.  n == 0 or odd gives 0; n > 32 gives
+ * PFB_ERR_SIZE (the reference throws, src/pfaffian.cu:44-45).  A zero pivot
+ * gives 0.  out: `batch` values of `dtype`.  No workspace.
+ */
+int pfb_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout,
+                 void *out, void *stream);
+
+/*
+ * (log|Pf|, sign) for any even n.
+ *
+ * Replaces the XLA handlers slog_pfaffian_f32 / _f64 / _c64 / _c128
+ * (bindings/jax_bindings.cu:19-80, symbols :115-150), which copy each matrix
+ * and run the host-driven loop of src/slog_pfaffian_lg.cu:151-211.
+ * log_out: `batch` doubles (pfcuda/cuda_api.py:78 declares the log as float64).
+ * sign_out: `batch` values of `dtype`: +-1 for real input, a unit-modulus
+ * phase for complex input, 0 when Pf = 0 (then log = -inf).  Odd n gives
+ * (-inf, 0).  n <= 32 is accepted too (the Python layer refuses it as the
+ * reference does, cuda_api.py:60-61).  f32 / c64 input is evaluated in FP64 /
+ * complex128.
+ * workspace: at least pfb_slog_workspace_bytes(dtype, batch, n, mode) bytes,
+ * 256-byte aligned.
+ */
+int pfb_slog_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout,
+                      int mode, double *log_out, void *sign_out,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+size_t pfb_slog_workspace_bytes(int dtype, int64_t batch, int n, int mode);
+
+/*
+ * Optional instrumentation for pfb_slog_pfaffian_timed: caller-created CUDA
+ * events (cudaEvent_t passed as void*), recorded on `stream` around each launch
+ * of the panel kernel and of the trailing-update kernel(s).  Entry 2i / 2i+1 of
+ * each array is the start / stop of the i-th panel (update); at most `pairs`
+ * pairs are recorded per array.  The number of panels is ceil((n-1)/nb) with
+ * nb = pfb_slog_panel_width(dtype, n).
+ */
+typedef struct {
+    void **panel_events;
+    void **update_events;
+    int pairs;
+} pfb_slog_timing;
+
+/* pfb_slog_pfaffian with event records around its kernels (timing may be NULL). */
+int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int layout,
+                            int mode, double *log_out, void *sign_out,
+                            void *workspace, size_t workspace_bytes, void *stream,
+                            const pfb_slog_timing *timing);
+
+/* Panel width (pivot rows per panel) the blocked factorisation uses for this
+ * dtype and order; 0 if the order is not supported. */
+int pfb_slog_panel_width(int dtype, int n);
+
+/*
+ * Pivot columns chosen by the last pfb_slog_pfaffian call that used this
+ * workspace: n/2 int32 per matrix (the column index swapped into position k+1
+ * at pivot step k, as the reference's argmax picks it).  Copies into the device
+ * buffer `piv_out` on `stream`.
+ */
+int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
+                    int32_t *piv_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFB200_H */

@@ -1,0 +1,187 @@
+"""Python API of the engine, mirroring pfcuda/cuda_api.py.
+
+``pfaffian(A)`` and ``slog_pfaffian(A)`` keep the reference's names, argument
+meaning, shape rules and error behaviour (pfcuda/cuda_api.py:27-76); the host
+framework here is PyTorch (JAX is not part of this engine's runtime), so inputs
+are torch tensors on a CUDA device, with any leading batch dimensions standing
+in for jax.vmap (the reference registers vmap_method='broadcast_all',
+cuda_api.py:51,73).  NumPy arrays are accepted too: they are copied to the
+current CUDA device and the result comes back as NumPy.
+
+Differentiation mirrors the reference's JVP rules (cuda_api.py:78-107): the
+tangent of log|Pf| is (1/2) tr(A^-1 dA) and the tangent of Pf is that times Pf.
+``slog_pfaffian`` is a torch.autograd.Function whose backward is the engine's
+adjoint kernel (pfcuda_b200.grad).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_DT = {
+    torch.float32: _lib.F32,
+    torch.float64: _lib.F64,
+    torch.complex64: _lib.C64,
+    torch.complex128: _lib.C128,
+}
+_MODES = {"fp64": _lib.MODE_FP64, "split": _lib.MODE_SPLIT}
+
+
+def _stream(t: torch.Tensor) -> int:
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def _prep(A):
+    """torch CUDA tensor (contiguous) and a flag telling to return NumPy."""
+    as_np = isinstance(A, np.ndarray)
+    if as_np:
+        A = torch.from_numpy(np.ascontiguousarray(A))
+    if not isinstance(A, torch.Tensor):
+        raise TypeError("expected a torch.Tensor or numpy.ndarray")
+    if A.ndim < 2 or A.shape[-1] != A.shape[-2]:
+        raise ValueError(f"expected (..., n, n) matrices, got shape {tuple(A.shape)}")
+    if A.dtype not in _DT:
+        raise TypeError(f"unsupported dtype {A.dtype}; use float32, float64, complex64 or complex128")
+    return A, as_np
+
+
+def _out(x, as_np):
+    return x.cpu().numpy() if as_np else x
+
+
+def _to_device(A, as_np):
+    """NumPy input goes to the current CUDA device; a CPU torch tensor is refused
+    (the engine has no CPU fallback)."""
+    if as_np:
+        return A.cuda()
+    if not A.is_cuda:
+        raise ValueError("the engine runs on CUDA tensors only (no CPU fallback)")
+    return A
+
+
+def pfaffian(A):
+    """Pf(A) for 2n <= 32 (pfcuda/cuda_api.py:27-54).
+
+    Odd or empty order gives 0; 2x2 and 4x4 use the closed forms (cuda_api.py:
+    34-42); orders above 32 raise ValueError (cuda_api.py:44-45).
+    """
+    A, as_np = _prep(A)
+    n = A.shape[-1]
+    if n == 0 or n & 1:
+        return _out(torch.zeros(A.shape[:-2], dtype=A.dtype, device=A.device), as_np)
+    if n == 2:
+        return _out(A[..., 0, 1].clone(), as_np)
+    if n == 4:
+        return _out(A[..., 0, 1] * A[..., 2, 3] - A[..., 0, 2] * A[..., 1, 3]
+                    + A[..., 0, 3] * A[..., 1, 2], as_np)
+    if n > 32:
+        raise ValueError("Matrix size exceeds the maximum supported size of 32x32.")
+    A = _to_device(A, as_np)
+    return _out(_PfaffianFn.apply(A.contiguous()), as_np)
+
+
+def slog_pfaffian(A, mode: str = "split"):
+    """(log|Pf(A)|, sign) for 2n > 32 (pfcuda/cuda_api.py:56-76).
+
+    Orders up to 32 raise ValueError (cuda_api.py:60-61); odd order returns
+    (-inf, 0) (cuda_api.py:63-67).  The log is float64 (cuda_api.py:71); the sign
+    has A's dtype (a unit-modulus phase for complex A, 0 when Pf = 0).
+    ``mode`` picks the arithmetic of the trailing update: "split" (int8 slices on
+    the tensor cores, recombined in FP64) or "fp64".
+    """
+    A, as_np = _prep(A)
+    n = A.shape[-1]
+    if n <= 32:
+        raise ValueError("Matrix size is less than the minimum supported size of (33x33). "
+                         "Use pfaffian() for smaller matrices.")
+    if n & 1:
+        lead = A.shape[:-2]
+        la = torch.full(lead, -float("inf"), dtype=torch.float64, device=A.device)
+        sg = torch.zeros(lead, dtype=A.dtype, device=A.device)
+        return _out(la, as_np), _out(sg, as_np)
+    if mode not in _MODES:
+        raise ValueError(f"mode must be one of {sorted(_MODES)}")
+    A = _to_device(A, as_np)
+    la, sg = _SlogFn.apply(A.contiguous(), mode)
+    return _out(la, as_np), _out(sg, as_np)
+
+
+# ------------------------------------------------------------------ raw calls
+
+def pfaffian_raw(A: torch.Tensor, layout: int = _lib.ROW_MAJOR) -> torch.Tensor:
+    """One pfb_pfaffian call on a contiguous (..., n, n) CUDA tensor (n <= 32)."""
+    n = A.shape[-1]
+    B = A.numel() // max(n * n, 1) if n else int(np.prod(A.shape[:-2]))
+    out = torch.empty(A.shape[:-2], dtype=A.dtype, device=A.device)
+    st = _lib.lib().pfb_pfaffian(_DT[A.dtype], A.data_ptr(), B, n, layout, out.data_ptr(), _stream(A))
+    _lib.check(st, "pfb_pfaffian")
+    return out
+
+
+def slog_workspace_bytes(dtype: torch.dtype, batch: int, n: int, mode: str = "split") -> int:
+    return int(_lib.lib().pfb_slog_workspace_bytes(_DT[dtype], batch, n, _MODES[mode]))
+
+
+def slog_pfaffian_raw(A: torch.Tensor, mode: str = "split", layout: int = _lib.ROW_MAJOR,
+                      workspace: torch.Tensor | None = None, return_pivots: bool = False):
+    """One pfb_slog_pfaffian call on a contiguous (..., n, n) CUDA tensor, any even n."""
+    n = A.shape[-1]
+    lead = A.shape[:-2]
+    B = int(np.prod(lead)) if len(lead) else 1
+    la = torch.empty(lead, dtype=torch.float64, device=A.device)
+    sg = torch.empty(lead, dtype=A.dtype, device=A.device)
+    wsb = slog_workspace_bytes(A.dtype, B, n, mode)
+    if workspace is None or workspace.numel() < wsb:
+        workspace = torch.empty(max(wsb, 1), dtype=torch.uint8, device=A.device)
+    st = _lib.lib().pfb_slog_pfaffian(_DT[A.dtype], A.data_ptr(), B, n, layout, _MODES[mode],
+                                      la.data_ptr(), sg.data_ptr(), workspace.data_ptr(), wsb,
+                                      _stream(A))
+    _lib.check(st, "pfb_slog_pfaffian")
+    if return_pivots:
+        piv = torch.empty(lead + (n // 2,), dtype=torch.int32, device=A.device)
+        st = _lib.lib().pfb_slog_pivots(B, n, workspace.data_ptr(), wsb, piv.data_ptr(), _stream(A))
+        _lib.check(st, "pfb_slog_pivots")
+        return la, sg, piv
+    return la, sg
+
+
+# ------------------------------------------------------------- autograd glue
+
+class _PfaffianFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, A):
+        pf = pfaffian_raw(A)
+        ctx.save_for_backward(A, pf)
+        return pf
+
+    @staticmethod
+    def backward(ctx, g):
+        # d Pf = (1/2) Pf tr(A^-1 dA)  (pfcuda/cuda_api.py:85-97), so
+        # dPf/dA_ij = (1/2) Pf (A^-1)_ji; torch wants conj of that for complex.
+        A, pf = ctx.saved_tensors
+        Ainv_t = torch.linalg.inv(A).transpose(-1, -2)
+        grad = 0.5 * (pf[..., None, None] * Ainv_t)
+        if A.is_complex():
+            grad = grad.conj()
+        return g[..., None, None] * grad
+
+
+class _SlogFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, A, mode):
+        la, sg = slog_pfaffian_raw(A, mode)
+        ctx.save_for_backward(A)
+        ctx.mode = mode
+        ctx.mark_non_differentiable(sg)
+        return la, sg
+
+    @staticmethod
+    def backward(ctx, g_log, g_sign):
+        from .grad import slog_pfaffian_grad
+        (A,) = ctx.saved_tensors
+        G = slog_pfaffian_grad(A)        # d log Pf / dA = (1/2) A^-T (holomorphic)
+        if A.is_complex():
+            G = G.conj()
+        return g_log[..., None, None].to(G.dtype) * G, None

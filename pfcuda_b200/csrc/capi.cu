@@ -1,0 +1,107 @@
+// capi.cu -- the extern "C" entry points declared in include/pfb200.h.
+//
+// Argument checking and dispatch only; the kernels live in small.cu and
+// large.cu.  Nothing here allocates device memory or synchronises the host.
+#include <string.h>
+
+#include "common.cuh"
+#include "small.cuh"
+#include "large.cuh"
+
+namespace {
+thread_local int g_last_cuda_error = 0;
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return PFB_OK;
+    g_last_cuda_error = (int)e;
+    return PFB_ERR_CUDA;
+}
+
+bool valid_dtype(int d) { return d == PFB_F32 || d == PFB_F64 || d == PFB_C64 || d == PFB_C128; }
+bool valid_layout(int l) { return l == PFB_ROW_MAJOR || l == PFB_COL_MAJOR; }
+}  // namespace
+
+extern "C" {
+
+const char *pfb_status_string(int status)
+{
+    switch (status) {
+    case PFB_OK: return "ok";
+    case PFB_ERR_INVALID: return "invalid argument";
+    case PFB_ERR_SIZE: return "matrix order outside the supported range";
+    case PFB_ERR_WORKSPACE: return "workspace missing, too small or misaligned";
+    case PFB_ERR_CUDA: return "CUDA runtime error";
+    case PFB_ERR_UNSUPPORTED: return "unsupported combination";
+    case PFB_ERR_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int pfb_last_cuda_error(void) { return g_last_cuda_error; }
+
+int pfb_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout, void *out, void *stream)
+{
+    if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
+    if (n > 32) return PFB_ERR_SIZE;
+    if (batch == 0) return PFB_OK;
+    if (!out || (!A && n > 0)) return PFB_ERR_INVALID;
+    int rc = pfb::launch_small(dtype, false, A, batch, n, layout, out, nullptr, nullptr,
+                               (cudaStream_t)stream);
+    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    return rc;
+}
+
+size_t pfb_slog_workspace_bytes(int dtype, int64_t batch, int n, int mode)
+{
+    if (!valid_dtype(dtype) || batch < 0 || n < 0) return 0;
+    return pfb::large_workspace_bytes(dtype, batch, n, mode);
+}
+
+int pfb_slog_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                      double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
+                      void *stream)
+{
+    return pfb_slog_pfaffian_timed(dtype, A, batch, n, layout, mode, log_out, sign_out, workspace,
+                                   workspace_bytes, stream, nullptr);
+}
+
+int pfb_slog_panel_width(int dtype, int n)
+{
+    if (!valid_dtype(dtype) || n < 0) return 0;
+    return pfb::large_panel_width(dtype, n);
+}
+
+int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                            double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
+                            void *stream, const pfb_slog_timing *timing)
+{
+    if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
+    if (mode != PFB_MODE_FP64 && mode != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
+    if (batch == 0) return PFB_OK;
+    if (!log_out || !sign_out || (!A && n > 0)) return PFB_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+    if (n <= 32 || (n & 1)) {
+        // odd orders give (-inf, 0) from the small kernel without reading A
+        rc = pfb::launch_small(dtype, true, A, batch, (n & 1) ? 1 : n, layout, nullptr, log_out,
+                               sign_out, s);
+    } else {
+        const size_t need = pfb::large_workspace_bytes(dtype, batch, n, mode);
+        if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u))
+            return PFB_ERR_WORKSPACE;
+        rc = pfb::launch_large(dtype, A, batch, n, layout, mode, log_out, sign_out, workspace,
+                               workspace_bytes, s, timing);
+    }
+    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    return rc;
+}
+
+int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
+                    int32_t *piv_out, void *stream)
+{
+    if (batch < 0 || n < 0 || !piv_out || !workspace) return PFB_ERR_INVALID;
+    return pfb::large_copy_pivots(batch, n, workspace, workspace_bytes, piv_out, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,32 @@
+// large.cuh -- blocked skew-LTL^T factorisation for (log|Pf|, sign) of large
+// matrices, see large.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/pfb200.h"
+
+namespace pfb {
+
+// Per-matrix running state of the factorisation, kept in the workspace.
+struct __align__(64) MatState {
+    double log_abs;   // sum of log|pivot|
+    double ph_re;     // product of pivot / |pivot| (imaginary part 0 for real input)
+    double ph_im;
+    int parity;       // number of interchanges mod 2
+    int dead;         // a zero pivot was met: Pf = 0
+};
+
+size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode);
+
+int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                 double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
+                 cudaStream_t stream, const pfb_slog_timing *timing);
+
+int large_panel_width(int dtype, int n);
+
+int large_copy_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
+                      int32_t *piv_out, cudaStream_t stream);
+
+}  // namespace pfb

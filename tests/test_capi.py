@@ -1,0 +1,64 @@
+"""The C-ABI library: symbols, status strings and argument checks (no GPU needed).
+
+Every call here returns before any CUDA work is enqueued.
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+from pfcuda_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pfb200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(pfb_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_functions()
+    assert len(names) >= 6
+    for name in names:
+        assert hasattr(L, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_status_strings():
+    L = _lib.lib()
+    for st in range(0, 8):
+        assert isinstance(L.pfb_status_string(st), bytes)
+    assert L.pfb_status_string(0) == b"ok"
+
+
+def test_argument_checks_without_gpu():
+    L = _lib.lib()
+    out = ctypes.c_double()
+    p = ctypes.addressof(out)
+    assert L.pfb_pfaffian(9, p, 1, 8, 0, p, None) == 1          # bad dtype
+    assert L.pfb_pfaffian(1, p, 1, 8, 7, p, None) == 1          # bad layout
+    assert L.pfb_pfaffian(1, p, -1, 8, 0, p, None) == 1         # negative batch
+    assert L.pfb_pfaffian(1, p, 1, 34, 0, p, None) == 2         # order above 32
+    assert L.pfb_pfaffian(1, p, 0, 8, 0, p, None) == 0          # empty batch
+    assert L.pfb_pfaffian(1, p, 1, 8, 0, None, None) == 1       # no output
+    assert L.pfb_slog_pfaffian(1, p, 1, 64, 0, 5, p, p, None, 0, None) == 1   # bad mode
+    assert L.pfb_slog_pfaffian(1, p, 1, 64, 0, 0, p, p, None, 0, None) == 3   # no workspace
+    assert L.pfb_slog_pfaffian(1, p, 0, 64, 0, 0, p, p, None, 0, None) == 0
+
+
+@pytest.mark.parametrize("dtype", [0, 1, 2, 3])
+def test_workspace_sizes(dtype):
+    L = _lib.lib()
+    prev = 0
+    for n in (34, 64, 128, 1024, 4096):
+        for mode in (0, 1):
+            w = L.pfb_slog_workspace_bytes(dtype, 1, n, mode)
+            assert w > 0 and w % 256 == 0
+        w = L.pfb_slog_workspace_bytes(dtype, 1, n, 0)
+        assert w >= prev
+        prev = w
+    assert L.pfb_slog_workspace_bytes(dtype, 2, 1024, 0) > L.pfb_slog_workspace_bytes(dtype, 1, 1024, 0)
+    assert L.pfb_slog_workspace_bytes(dtype, 1, 1 << 20, 0) == 0   # beyond the supported order

@@ -1,0 +1,165 @@
+"""Large path (pfb_slog_pfaffian, blocked skew-LTL^T) against the oracle.
+
+Bar (the engine's accuracy target): |log|Pf| - oracle| <= 1e-10 * |log|Pf||
+(plus 1e-12 absolute for logs near 0), the sign identical (real) or the phase
+within 1e-10 (complex), and the pivot columns identical to the oracle's.
+"""
+import numpy as np
+import pytest
+import torch
+
+import pfcuda_b200 as pf
+from pfcuda_b200 import _lib
+from oracle import oracle as O
+from golden_io import load, split
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["fp64"]
+
+
+def cuda(a):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def check(A, mode, pivots=True, tol=1e-10):
+    la, sg, piv = pf.slog_pfaffian_raw(cuda(A), mode=mode, return_pivots=True)
+    la, sg, piv = la.cpu().numpy(), sg.cpu().numpy(), piv.cpu().numpy()
+    wl, ws, wp = O.slog_pf(A, with_pivots=True)
+    err = np.abs(la - wl)
+    assert np.all(err <= tol * np.abs(wl) + 1e-12), (A.shape, err.max())
+    if np.iscomplexobj(A):
+        assert np.all(np.abs(sg - ws) <= 1e-10)
+    else:
+        assert np.array_equal(sg, ws)
+    if pivots:
+        assert np.array_equal(piv, wp)
+    return la, sg
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [34, 36, 40, 62, 64, 66, 100, 126, 128, 130, 192, 200, 256, 290])
+def test_orders_f64(mode, n):
+    rng = np.random.default_rng(n)
+    check(O.skew_normal(rng, 3, n, scale=1 / np.sqrt(n)), mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [34, 64, 66, 100, 256])
+def test_orders_c128(mode, n):
+    rng = np.random.default_rng(n + 1)
+    check(O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n), complex_=True), mode)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("npdt", [np.float32, np.complex64])
+def test_single_precision_inputs_run_in_fp64(mode, npdt):
+    rng = np.random.default_rng(4)
+    A = O.skew_normal(rng, 2, 96, scale=0.1, complex_=np.dtype(npdt).kind == "c").astype(npdt)
+    la, sg, piv = pf.slog_pfaffian_raw(cuda(A), mode=mode, return_pivots=True)
+    wl, ws, wp = O.slog_pf(A)       # the oracle upcasts the same values
+    assert np.all(np.abs(la.cpu().numpy() - wl) <= 1e-10 * np.abs(wl))
+    assert np.all(np.abs(sg.cpu().numpy() - ws) <= 1e-6)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [64, 130, 258])
+def test_column_major_layout(mode, n):
+    rng = np.random.default_rng(n)
+    for cplx in (False, True):
+        A = O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n), complex_=cplx)
+        At = np.ascontiguousarray(np.swapaxes(A, -1, -2))
+        l1, s1 = pf.slog_pfaffian_raw(cuda(A), mode=mode)
+        l2, s2 = pf.slog_pfaffian_raw(cuda(At), mode=mode, layout=_lib.COL_MAJOR)
+        assert torch.equal(l1, l2) and torch.equal(s1, s2)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_zero_and_singular(mode):
+    for n in range(34, 68, 8):
+        la, sg = pf.slog_pfaffian(cuda(np.zeros((n, n))), mode=mode)
+        assert np.isneginf(la.item()) and sg.item() == 0
+    rng = np.random.default_rng(2)
+    A = O.skew_normal(rng, 3, 80, scale=0.1)
+    A[1, 17, :] = 0
+    A[1, :, 17] = 0
+    la, sg = pf.slog_pfaffian_raw(cuda(A), mode=mode)
+    la = la.cpu().numpy()
+    assert np.isneginf(la[1]) and sg[1].item() == 0 and np.isfinite(la[0]) and np.isfinite(la[2])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_reference_det_relation(mode):
+    rng = np.random.default_rng(1)                 # test/slog_pfaffian_test.py:47-59
+    for n in range(34, 66, 2):
+        G = rng.normal(size=(n, n))
+        A = G - G.T
+        la, sg = pf.slog_pfaffian(cuda(A), mode=mode)
+        assert np.isclose(np.exp(2 * la.item()), np.linalg.det(A), rtol=1e-8, atol=1e-10)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_reference_random_and_identity(mode):
+    rng = np.random.default_rng(123)               # test/slog_pfaffian_test.py:61-74
+    for n in range(40, 300, 10):
+        G = rng.normal(size=(3, n, n))
+        A = G - np.swapaxes(G, -1, -2)
+        la, sg = pf.slog_pfaffian_raw(cuda(A), mode=mode)
+        wl, ws = O.slog_pf(A)
+        np.testing.assert_allclose(sg.cpu().numpy() * np.exp(la.cpu().numpy() - wl), ws, rtol=1e-8)
+    g = load("known.npz")                          # test/slog_pfaffian_test.py:76-107
+    for A, want in zip(split(g["A"], g["n"]), g["pf"]):
+        if A.shape[0] <= 32:
+            continue
+        la, sg = pf.slog_pfaffian(cuda(A), mode=mode)
+        assert np.isclose(sg.item() * np.exp(la.item()), want, rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_reference_cpu_large_values(mode):
+    g = load("cpu_large.npz")
+    for seed, n, want in zip(g["seeds"], g["n"], g["pf"]):
+        A = O.config_large(int(n), seed=int(seed))
+        la, sg = pf.slog_pfaffian(cuda(A), mode=mode)
+        assert abs(la.item() - np.log(abs(want))) <= 1e-10 * abs(la.item())
+        assert sg.item() == np.sign(want)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_and_input_untouched(mode):
+    rng = np.random.default_rng(6)
+    A = O.skew_normal(rng, 5, 300, scale=0.05)
+    X = cuda(A)
+    X0 = X.clone()
+    la, sg = pf.slog_pfaffian_raw(X, mode=mode)
+    assert torch.equal(X, X0)
+    for b in range(5):
+        l1, s1 = pf.slog_pfaffian_raw(X[b], mode=mode)
+        assert l1.item() == la[b].item() and s1.item() == sg[b].item()
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("n", [1024, 2048])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_benchmark_orders(mode, n, cplx):
+    A = O.config_large(n, dtype=np.complex128 if cplx else np.float64, seed=1)
+    check(A, mode, pivots=not cplx)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_order_4096_f64(mode):
+    A = O.config_large(4096, seed=1)
+    la, sg = pf.slog_pfaffian(cuda(A), mode=mode)
+    s, ld = np.linalg.slogdet(A[0])
+    assert abs(2 * la.item() - ld) <= 1e-10 * abs(ld)
+    assert s > 0
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_ill_conditioned(mode):
+    A, logs, signs = O.config_illcond(seed=4, B=2, n=256)
+    la, sg = pf.slog_pfaffian(cuda(A), mode=mode)
+    la, sg = la.cpu().numpy(), sg.cpu().numpy()
+    assert np.all(np.abs(la - logs) <= 1e-10 * np.abs(logs))
+    assert np.array_equal(sg, signs)
