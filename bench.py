@@ -39,7 +39,7 @@ N_DEFAULT = 4096
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--n", type=int, default=N_DEFAULT)
@@ -73,10 +73,14 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10:   # sampling has begun
+                time.sleep(0.01)
+            self.lines.clear()
         except OSError:
             self.proc = None
 
@@ -121,7 +125,7 @@ def run_reference(args, rank, world):
     if R is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cpu.so was not built"}))
         return
-    threads = os.cpu_count() or 1
+    threads = min(os.cpu_count() or 1, 32)
     n = args.n
     A = O.config_large(n, seed=1)[0]
     batch = np.ascontiguousarray(np.broadcast_to(A, (threads, n, n)))
@@ -156,7 +160,7 @@ def cpu_baseline(n):
     R = O.ref_cpu()
     if R is None:
         return None
-    threads = os.cpu_count() or 1
+    threads = min(os.cpu_count() or 1, 32)
     A = O.config_large(n, seed=1)[0]
     batch = np.ascontiguousarray(np.broadcast_to(A, (threads, n, n)))
     out = np.empty(threads)
@@ -275,11 +279,13 @@ def main():
     nb = L.pfb_slog_panel_width(dtc, n)
     npan = (n - 1 + nb - 1) // nb
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * npan)] for _ in range(2)]
+    for e in evs[0] + evs[1]:
+        e.record(stream)          # creates the CUDA events (torch creates them lazily)
+    torch.cuda.synchronize()
     arr = [(ctypes.c_void_p * (2 * npan))(*[e.cuda_event for e in es]) for es in evs]
+    assert all(e.cuda_event for e in evs[0] + evs[1])
     tm = _lib.SlogTiming(ctypes.cast(arr[0], ctypes.POINTER(ctypes.c_void_p)),
                          ctypes.cast(arr[1], ctypes.POINTER(ctypes.c_void_p)), npan)
-    for e in evs[0] + evs[1]:
-        e.record(stream)          # every event is recorded at least once
     st = L.pfb_slog_pfaffian_timed(dtc, A.data_ptr(), 1, n, _lib.ROW_MAJOR, mc[head], la.data_ptr(),
                                    sg.data_ptr(), ws[head].data_ptr(), ws[head].numel(),
                                    stream.cuda_stream, ctypes.byref(tm))

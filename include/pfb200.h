@@ -49,6 +49,10 @@ typedef enum {
     PFB_MODE_SPLIT = 1   /* error-free int8 slices on the tcgen05 tensor cores with
                             exact int32 accumulation, recombined in FP64             */
 } pfb_mode;
+/* For PFB_MODE_SPLIT, bits 8..11 of `mode` may give the number of 7-bit int8
+ * digits per operand (1..7; 0 selects the default, 7).  Fewer digits trade
+ * accuracy for speed: S digits keep the update to about K * 2^(-7S) relative. */
+#define PFB_SPLIT_DIGITS(s) ((s) << 8)
 
 typedef enum {
     PFB_OK = 0,

@@ -55,6 +55,7 @@ int pfb_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout, voi
 size_t pfb_slog_workspace_bytes(int dtype, int64_t batch, int n, int mode)
 {
     if (!valid_dtype(dtype) || batch < 0 || n < 0) return 0;
+    if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return 0;
     return pfb::large_workspace_bytes(dtype, batch, n, mode);
 }
 
@@ -77,7 +78,8 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
                             void *stream, const pfb_slog_timing *timing)
 {
     if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
-    if (mode != PFB_MODE_FP64 && mode != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
+    if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
+    if ((mode & ~0xfff) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
     if (batch == 0) return PFB_OK;
     if (!log_out || !sign_out || (!A && n > 0)) return PFB_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;

@@ -143,7 +143,7 @@ static LargeLayout large_layout(int dtype, int64_t B, int n, int mode)
     L.w_off = off;
     off = align256(off + (size_t)B * (size_t)n * (size_t)n * ts);
     L.split_off = off;
-    if (mode == PFB_MODE_SPLIT) off = align256(off + split_workspace_bytes(cplx, B, n, nb));
+    if ((mode & 0xff) == PFB_MODE_SPLIT) off = align256(off + split_workspace_bytes(cplx, B, n, nb));
     L.total = off;
     return L;
 }
@@ -573,13 +573,20 @@ gemm_fp64_kernel(T *__restrict__ W_all, int n, int k0, int K, const MatState *__
 
 // ----------------------------------------------------------------- finalize
 
+// A device-side timeout of the update kernel (err != 0) yields log = NaN.
 template <typename T>
-__global__ void finalize_kernel(const MatState *__restrict__ st, int64_t batch, int negate,
-                                double *__restrict__ log_out, T *__restrict__ sign_out)
+__global__ void finalize_kernel(const MatState *__restrict__ st, const int32_t *__restrict__ err,
+                                int64_t batch, int negate, double *__restrict__ log_out,
+                                T *__restrict__ sign_out)
 {
     const int64_t bidx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (bidx >= batch) return;
     const MatState s = st[bidx];
+    if (err && err[bidx]) {
+        log_out[bidx] = NAN;
+        sign_out[bidx] = zero<T>();
+        return;
+    }
     if (s.dead) {
         log_out[bidx] = -INFINITY;
         sign_out[bidx] = zero<T>();
@@ -654,6 +661,12 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
 
     SplitArgs sa{};
     unsigned char *split_ws = ws + L.split_off;
+    const int slices = ((mode >> 8) & 0xf) ? ((mode >> 8) & 0xf) : kSplitDefaultSlices;
+    int32_t *split_err = nullptr;
+    if ((mode & 0xff) == PFB_MODE_SPLIT) {
+        split_err = split_args(true, split_ws, cplx, B, n, NB, 0, slices).err;
+        if (cudaMemsetAsync(split_err, 0, (size_t)B * sizeof(int32_t), s) != cudaSuccess) return PFB_ERR_CUDA;
+    }
     auto rec = [&](void **evs, int i) {
         if (tm && evs && i < 2 * tm->pairs) cudaEventRecord((cudaEvent_t)evs[i], s);
     };
@@ -664,8 +677,8 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
         int CL = mt > 0 ? (mt + kTT * CPT - 1) / (kTT * CPT) : 1;
         if (CL < 1) CL = 1;
         if (CL > kClusterMax) return PFB_ERR_SIZE;
-        const bool use_split = mode == PFB_MODE_SPLIT && mt > 0;
-        sa = split_args(use_split, split_ws, cplx, B, n, NB, k0);
+        const bool use_split = (mode & 0xff) == PFB_MODE_SPLIT && mt > 0;
+        sa = split_args(use_split, split_ws, cplx, B, n, NB, k0, slices);
 
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)CL, (unsigned)B, 1);
@@ -701,10 +714,10 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
     const int negate = (layout == PFB_COL_MAJOR) ? ((n >> 1) & 1) : 0;
     const unsigned fb = (unsigned)((B + 127) / 128);
     switch (dtype) {
-    case PFB_F32: finalize_kernel<float><<<fb, 128, 0, s>>>(st, B, negate, log_out, (float *)sign_out); break;
-    case PFB_F64: finalize_kernel<double><<<fb, 128, 0, s>>>(st, B, negate, log_out, (double *)sign_out); break;
-    case PFB_C64: finalize_kernel<c64><<<fb, 128, 0, s>>>(st, B, negate, log_out, (c64 *)sign_out); break;
-    default: finalize_kernel<c128><<<fb, 128, 0, s>>>(st, B, negate, log_out, (c128 *)sign_out); break;
+    case PFB_F32: finalize_kernel<float><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (float *)sign_out); break;
+    case PFB_F64: finalize_kernel<double><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (double *)sign_out); break;
+    case PFB_C64: finalize_kernel<c64><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (c64 *)sign_out); break;
+    default: finalize_kernel<c128><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (c128 *)sign_out); break;
     }
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
@@ -715,7 +728,7 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
 {
     int nb = 0, cpt = 0;
     if (!large_cfg(dtype, n, &nb, &cpt)) return PFB_ERR_SIZE;
-    if (mode == PFB_MODE_SPLIT && !split_available()) return PFB_ERR_UNSUPPORTED;
+    if ((mode & 0xff) == PFB_MODE_SPLIT && !split_available()) return PFB_ERR_UNSUPPORTED;
     if (batch > 65535) return PFB_ERR_SIZE;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
     const bool cplx = dtype == PFB_C64 || dtype == PFB_C128;

@@ -11,27 +11,53 @@ namespace pfb {
 
 struct MatState;
 
-// Everything the panel kernel needs to write the slices of its Gauss vectors.
+constexpr int kSplitMaxSlices = 7;
+constexpr int kSplitDefaultSlices = 7;
+constexpr int kSplitTileM = 128;   // rows of an operand chunk (the MMA M)
+
+// Everything the panel kernel needs to write the int8 operands of the update.
+//
+// Operand layout: for slice s and 128-row tile t of the trailing index, one
+// contiguous chunk of 128 * kk bytes in the tcgen05 "K-major, no swizzle"
+// canonical form: core matrices of 8 rows x 16 bytes (128 contiguous bytes),
+// the core matrix of row group g and K-group kc at byte (g * kk/16 + kc) * 128.
+// A chunk is therefore the exact shared-memory image of an MMA operand tile and
+// moves with one bulk copy.
 struct SplitArgs {
     int enabled;
     int n, k0, nb, kk;        // kk = K of the int8 products (nb real, 2*nb complex)
-    int slices;               // number of 7-bit slices per operand
-    int64_t mstride;          // elements per matrix in xs / ys (= slices * n * kk)
-    int8_t *xs;               // [B][slices][n][kk]  A operand, K-major, rows = trailing index
-    int8_t *ys;               // [B][slices][n][kk]  B operand
+    int slices;               // digits per operand (<= kSplitMaxSlices)
+    int ntile;                // 128-row tiles covering the trailing index range
+    int cplx;
+    int64_t mstride;          // bytes per matrix of one operand array
+    int8_t *xs;               // A operand: [B][slices][ntile][128 * kk]
+    int8_t *ys;               // B operand (real: Y; complex: [Yr | -Yi])
+    int8_t *ys2;              // complex only: [Yi | Yr]
     int32_t *ex;              // [B][n] power-of-two exponent per trailing index
+    int32_t *err;             // [B] device-side timeout flags of the update kernel
 };
 
 size_t split_workspace_bytes(bool cplx, int64_t batch, int n, int nb);
-SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int n, int nb, int k0);
+SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int n, int nb, int k0,
+                     int slices);
 bool split_available();
 int launch_split_update(bool cplx, void *W, int n, int k0, int K, int64_t batch,
-                        const MatState *st, const SplitArgs &sa, cudaStream_t stream);
+                        MatState *st, const SplitArgs &sa, cudaStream_t stream);
+
+PFB_D void split_store16(int8_t *base, const SplitArgs &sa, int64_t b, int s, int ar, int kc,
+                         const int8_t (&d)[16])
+{
+    const int tile = ar >> 7, i = ar & 127, g = i >> 3, r = i & 7;
+    int8_t *p = base + b * sa.mstride +
+                ((int64_t)s * sa.ntile + tile) * (int64_t)(kSplitTileM * sa.kk) +
+                (g * (sa.kk >> 4) + kc) * 128 + r * 16;
+    *reinterpret_cast<int4 *>(p) = *reinterpret_cast<const int4 *>(d);
+}
 
 // Slice one trailing column's K panel values into `slices` int8 digits with a
-// shared power-of-two scale (error-free: every digit and remainder is exact in
-// FP64).  Y's digits are X's with each (u, w) pair mapped to (w, -u).  R is
-// consumed (overwritten by the remainders).
+// shared power-of-two scale (Ozaki's error-free splitting: every digit and
+// every remainder is exact in FP64).  Y's digits are X's with each (u, w) pair
+// mapped to (w, -u).  R is consumed (overwritten by the remainders).
 template <typename T, int NB>
 PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R)[NB], int K)
 {
@@ -53,35 +79,63 @@ PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R
         if constexpr (IsComplex<T>::value) { R[r].re *= sc; R[r].im *= sc; }
         else R[r] *= sc;
     }
-    constexpr int KK = IsComplex<T>::value ? 2 * NB : NB;
     for (int s = 0; s < sa.slices; s++) {
-        int8_t *xd = sa.xs + b * sa.mstride + ((int64_t)s * sa.n + a) * sa.kk;
-        int8_t *yd = sa.ys + b * sa.mstride + ((int64_t)s * sa.n + a) * sa.kk;
+        if constexpr (!IsComplex<T>::value) {
 #pragma unroll
-        for (int r0 = 0; r0 < KK; r0 += 16) {
-            alignas(16) int8_t dx[16], dy[16];
+            for (int kc = 0; kc < NB / 16; kc++) {
+                alignas(16) int8_t dx[16];
+                alignas(16) int8_t dy[16];
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                double v;
-                if constexpr (IsComplex<T>::value) v = ((r0 + r) < NB ? R[r0 + r].re : R[r0 + r - NB].im);
-                else v = R[r0 + r];
-                v *= 128.0;
-                const double d = trunc(v);
-                if constexpr (IsComplex<T>::value) {
-                    if ((r0 + r) < NB) R[r0 + r].re = v - d; else R[r0 + r - NB].im = v - d;
-                } else {
-                    R[r0 + r] = v - d;
+                for (int r = 0; r < 16; r++) {
+                    const double v = R[16 * kc + r] * 128.0;
+                    const double d = trunc(v);
+                    R[16 * kc + r] = v - d;
+                    dx[r] = (int8_t)d;
                 }
-                dx[r] = (int8_t)d;
-            }
-            // X = [Re | Im] per column; Y pairs (u, w) -> (w, -u)
 #pragma unroll
-            for (int r = 0; r < 16; r += 2) {
-                dy[r] = dx[r + 1];
-                dy[r + 1] = (int8_t)(-dx[r]);
+                for (int r = 0; r < 16; r += 2) {   // (u, w) -> (w, -u)
+                    dy[r] = dx[r + 1];
+                    dy[r + 1] = (int8_t)(-dx[r]);
+                }
+                split_store16(sa.xs, sa, b, s, col_rel, kc, dx);
+                split_store16(sa.ys, sa, b, s, col_rel, kc, dy);
             }
-            *reinterpret_cast<int4 *>(xd + r0) = *reinterpret_cast<const int4 *>(dx);
-            *reinterpret_cast<int4 *>(yd + r0) = *reinterpret_cast<const int4 *>(dy);
+        } else {
+            // A = [Xr | Xi],  B1 = [Yr | -Yi],  B2 = [Yi | Yr]:  Re = A.B1, Im = A.B2
+#pragma unroll
+            for (int kc = 0; kc < NB / 16; kc++) {
+                alignas(16) int8_t xr[16];
+                alignas(16) int8_t xi[16];
+                alignas(16) int8_t yr[16];
+                alignas(16) int8_t yi[16];
+                alignas(16) int8_t t[16];
+#pragma unroll
+                for (int r = 0; r < 16; r++) {
+                    double v = R[16 * kc + r].re * 128.0;
+                    double d = trunc(v);
+                    R[16 * kc + r].re = v - d;
+                    xr[r] = (int8_t)d;
+                    v = R[16 * kc + r].im * 128.0;
+                    d = trunc(v);
+                    R[16 * kc + r].im = v - d;
+                    xi[r] = (int8_t)d;
+                }
+#pragma unroll
+                for (int r = 0; r < 16; r += 2) {
+                    yr[r] = xr[r + 1];
+                    yr[r + 1] = (int8_t)(-xr[r]);
+                    yi[r] = xi[r + 1];
+                    yi[r + 1] = (int8_t)(-xi[r]);
+                }
+                split_store16(sa.xs, sa, b, s, col_rel, kc, xr);
+                split_store16(sa.xs, sa, b, s, col_rel, NB / 16 + kc, xi);
+                split_store16(sa.ys, sa, b, s, col_rel, kc, yr);
+#pragma unroll
+                for (int r = 0; r < 16; r++) t[r] = (int8_t)(-yi[r]);
+                split_store16(sa.ys, sa, b, s, col_rel, NB / 16 + kc, t);
+                split_store16(sa.ys2, sa, b, s, col_rel, kc, yi);
+                split_store16(sa.ys2, sa, b, s, col_rel, NB / 16 + kc, yr);
+            }
         }
     }
 }
