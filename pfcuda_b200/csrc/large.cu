@@ -188,21 +188,98 @@ struct PanelSmem {
     using Real = typename RealOf<T>::type;
     static constexpr int NT = kTT;
     static constexpr int NW = NT / 32;
-    T lb[NB][NB + 1];                       // replicated NB x NB block of panel columns
-    T rec[2][kClusterMax][NB + 1];          // pushed candidates: [0] value, [1..NB] column
-    Real rkey[2][kClusterMax];
-    int rcol[2][kClusterMax];
-    T stage[NW][NB + 1];                    // per-warp best candidate
+    T lb[NB][NB + 1];                  // replicated NB x NB block of the panel columns
+    alignas(16) T stage[2][NB];        // this CTA's best trailing column, panel rows 0..NB-1
+    T hval[2][kClusterMax];            // per-CTA best candidate, pushed by every CTA of the cluster
+    Real hkey[2][kClusterMax];
+    int hcol[2][kClusterMax];
+    T wval[NW];                        // per-warp best candidate
     Real wkey[NW];
     int wcol[NW];
+    T pivval[NB / 2];                  // this panel's pivots and pivot columns
+    int pivcol[NB / 2];
 };
 
 template <typename T> PFB_D void put(uint32_t a, T v) { st_remote(a, v); }
+PFB_D void store_pair(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
+PFB_D void store_pair(c128 *p, c128 a, c128 b) { p[0] = a; p[1] = b; }
+
+// s + sum over the window's Gauss-vector pairs (window pair index P >= fin0,
+// pair u = P - fin0) of  c_u[u] * Rw[2P+1] - c_w[u] * Rw[2P]  with
+// c_u = lb[2u][col], c_w = lb[2u+1][col].  Four partial sums shorten the
+// dependency chain; chunks of 8 pairs with a compiler barrier between them keep
+// the coefficient loads from all being hoisted into registers at once.
+template <typename T, int NB>
+PFB_D T lazy_row(T s, const T (&Rw)[NB], const T (*lb)[NB + 1], int col, int fin0)
+{
+    T s2 = zero<T>(), s3 = zero<T>(), s4 = zero<T>();
+#pragma unroll
+    for (int P0 = 0; P0 < NB / 2; P0 += 8) {
+        if (P0 + 7 >= fin0) {
+#pragma unroll
+            for (int P = P0; P < P0 + 8; P++) {
+                if (P >= 1 && P >= fin0) {
+                    const int u = P - fin0;
+                    if (P & 1) {
+                        s = fma_(lb[2 * u][col], Rw[2 * P + 1], s);
+                        s2 = fms_(lb[2 * u + 1][col], Rw[2 * P], s2);
+                    } else {
+                        s3 = fma_(lb[2 * u][col], Rw[2 * P + 1], s3);
+                        s4 = fms_(lb[2 * u + 1][col], Rw[2 * P], s4);
+                    }
+                }
+            }
+        }
+        asm volatile("" ::: "memory");
+    }
+    return (s + s2) + (s3 + s4);
+}
+
+// Interchange window rows 1 and p (2 <= p < NB, uniform across the CTA) with
+// a branch per position, so every register index stays static.
+template <typename T, int NB>
+PFB_D void swap_window_row(T (&Rw)[NB], int p)
+{
+    static_for<2, NB, 1>([&](auto pc) {
+        constexpr int P = decltype(pc)::value;
+        if (p == P) {
+            const T tmp = Rw[1];
+            Rw[1] = Rw[P];
+            Rw[P] = tmp;
+        }
+    });
+}
+
+PFB_D double ld_remote(uint32_t addr, double *)
+{
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+PFB_D c128 ld_remote(uint32_t addr, c128 *)
+{
+    double re, im;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(re), "=d"(im) : "r"(addr) : "memory");
+    return mk(re, im);
+}
 
 // Factor panel rows [k0, k0+NB) of every matrix; one cluster of CL CTAs per
 // matrix (blockIdx.y).  Thread i of CTA rank r keeps trailing columns
 // k0+NB + r*kTT + i + q*CL*kTT (q < CPT) of the panel rows in registers; threads
 // i < NB also own panel column k0+i, whose entries live in the shared block lb.
+//
+// The register window is rotated by two rows per pivot step, so the current
+// pivot rows are always Rw[0] (row k) and Rw[1] (row k+1) and the step loop
+// stays a loop (a fully unrolled panel does not fit the instruction cache).  At
+// step t, window position p holds panel row 2t+p for p < NB-2t (rows not yet
+// factored) and panel row p-(NB-2t) otherwise (the Gauss vectors of pairs
+// 0..t-1, u_s at even and w_s at odd positions).
+//
+// A pivot step costs one cluster barrier: every CTA pushes the header of its
+// best candidate (|value|, column, value) into every CTA's shared memory before
+// it, and the owner of a CTA's best trailing column stages that column; after
+// the barrier each CTA knows the pivot, and the panel-column threads read the
+// interchanged column straight from the winning CTA's stage.
 template <typename T, int NB, int CPT>
 __global__ void __launch_bounds__(kTT, 1)
 panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all,
@@ -210,7 +287,6 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
 {
     using Real = typename RealOf<T>::type;
     using SM = PanelSmem<T, NB>;
-    constexpr int NT = SM::NT;
     constexpr int NW = SM::NW;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM &sm = *reinterpret_cast<SM *>(smem_raw);
@@ -235,13 +311,13 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
 #pragma unroll
     for (int q = 0; q < CPT; q++) cq[q] = k1 + (int)rank * kTT + tid + q * GT;
 
-    // ---- load the panel rows
-    T R[CPT][NB];
+    // ---- load the panel rows (window position p = panel row p at step 0)
+    T Rw[CPT][NB];
 #pragma unroll
     for (int q = 0; q < CPT; q++)
 #pragma unroll
         for (int r = 0; r < NB; r++)
-            R[q][r] = (cq[q] < n && k0 + r < n) ? W[(int64_t)(k0 + r) * n + cq[q]] : zero<T>();
+            Rw[q][r] = (cq[q] < n && k0 + r < n) ? W[(int64_t)(k0 + r) * n + cq[q]] : zero<T>();
     if (has_panel) {
         for (int r = 0; r < NB; r++)
             sm.lb[r][tid] = (k0 + r < n && pc < n) ? W[(int64_t)(k0 + r) * n + pc] : zero<T>();
@@ -257,31 +333,25 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
         parity = st->parity;
     }
     bool dead = false;
+    const int nsteps = (n - k0) / 2 < NB / 2 ? (n - k0) / 2 : NB / 2;
     // every CTA of the cluster has started (and loaded) before any shared
     // memory of another CTA is written
     cluster_sync();
 
-    static_for<0, NB / 2, 1>([&](auto tc) {
-        constexpr int t = decltype(tc)::value;
+    int t = 0;
+#pragma unroll 1
+    for (; t < nsteps; t++) {
         const int k = k0 + 2 * t;
-        if (dead || k >= n - 1) return;   // uniform
+        const int par = t & 1;
+        const int fin0 = NB / 2 - t;   // window pair index of the oldest Gauss-vector pair
 
         // (1) lazy update of row k with the panel's earlier Gauss vectors
 #pragma unroll
-        for (int q = 0; q < CPT; q++) {
-            T s = R[q][2 * t];
-#pragma unroll
-            for (int u = 0; u < t; u++) {
-                s = fma_(sm.lb[2 * u][2 * t], R[q][2 * u + 1], s);
-                s = fms_(sm.lb[2 * u + 1][2 * t], R[q][2 * u], s);
-            }
-            R[q][2 * t] = s;
-        }
+        for (int q = 0; q < CPT; q++) Rw[q][0] = lazy_row<T, NB>(Rw[q][0], Rw[q], sm.lb, 2 * t, fin0);
         const bool pcand = has_panel && tid > 2 * t && pc < n;
         T pv = zero<T>();
         if (pcand) {
             T s = sm.lb[2 * t][tid];
-#pragma unroll
             for (int u = 0; u < t; u++) {
                 s = fma_(sm.lb[2 * u][2 * t], sm.lb[2 * u + 1][tid], s);
                 s = fms_(sm.lb[2 * u + 1][2 * t], sm.lb[2 * u][tid], s);
@@ -290,7 +360,7 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             pv = s;
         }
 
-        // (2) this thread's best candidate (panel column first: it is the
+        // (2) this thread's best candidate (its panel column first: the
         // smaller index), then the warp's
         Real key = (Real)(-1);
         int col = INT_MAX;
@@ -300,8 +370,8 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             if (cq[q] < n) {
-                Real kq = pkey(R[q][2 * t]);
-                if (kq > key) { key = kq; col = cq[q]; qsel = q; val = R[q][2 * t]; }
+                Real kq = pkey(Rw[q][0]);
+                if (kq > key) { key = kq; col = cq[q]; qsel = q; val = Rw[q][0]; }
             }
         }
         Real wk = key;
@@ -312,22 +382,12 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             int c2 = shfl_xor(wc, off);
             if (k2 > wk || (k2 == wk && c2 < wc)) { wk = k2; wc = c2; }
         }
-        if (wc != INT_MAX && col == wc) {   // this thread owns the warp's best column
-            sm.stage[warp][0] = val;
-            if (qsel >= 0) {
-#pragma unroll
-                for (int r = 0; r < NB; r++) {
-                    T v = R[0][r];
-#pragma unroll
-                    for (int q = 1; q < CPT; q++) v = (qsel == q) ? R[q][r] : v;
-                    sm.stage[warp][1 + r] = v;
-                }
-            }
-        }
+        if (wc != INT_MAX && col == wc) sm.wval[warp] = val;
         if (lane == 0) { sm.wkey[warp] = wk; sm.wcol[warp] = wc; }
         __syncthreads();
 
-        // (3) the CTA's best candidate, pushed into every CTA of the cluster
+        // (3) the CTA's best candidate: its header goes to every CTA of the
+        // cluster, and if it is a trailing column its owner stages the column
         Real ck = (Real)(-1);
         int cc = INT_MAX, cw = 0;
 #pragma unroll
@@ -336,48 +396,66 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             int c = sm.wcol[w];
             if (kk > ck || (kk == ck && c < cc)) { ck = kk; cc = c; cw = w; }
         }
-        constexpr int buf = t & 1;
         if (tid < CL) {
-            put(map_rank(smem_u32(&sm.rkey[buf][rank]), tid), ck);
-            put(map_rank(smem_u32(&sm.rcol[buf][rank]), tid), cc);
+            put(map_rank(smem_u32(&sm.hkey[par][rank]), tid), ck);
+            put(map_rank(smem_u32(&sm.hcol[par][rank]), tid), cc);
+            put(map_rank(smem_u32(&sm.hval[par][rank]), tid), sm.wval[cw]);
         }
-        {
-            const int nv = (cc != INT_MAX && cc >= k1) ? NB + 1 : 1;
-            for (int idx = tid; idx < CL * nv; idx += NT) {
-                const int dst = idx / nv, e = idx - dst * nv;
-                put(map_rank(smem_u32(&sm.rec[buf][rank][e]), dst), sm.stage[cw][e]);
+        if (qsel >= 0 && col == cc) {
+#pragma unroll
+            for (int P = 0; P < NB / 2; P++) {
+                // window pair P holds panel rows (r, r+1), r even
+                const int r = (2 * P < NB - 2 * t) ? 2 * t + 2 * P : 2 * P - (NB - 2 * t);
+                T v0 = Rw[0][2 * P], v1 = Rw[0][2 * P + 1];
+#pragma unroll
+                for (int q = 1; q < CPT; q++) {
+                    v0 = (qsel == q) ? Rw[q][2 * P] : v0;
+                    v1 = (qsel == q) ? Rw[q][2 * P + 1] : v1;
+                }
+                store_pair(&sm.stage[par][r], v0, v1);
             }
         }
         cluster_sync();
 
-        // (4) the pivot
-        Real gk = (Real)(-1);
-        int j = INT_MAX, gs = 0;
-        for (int s2 = 0; s2 < CL; s2++) {
-            Real kk = sm.rkey[buf][s2];
-            int c = sm.rcol[buf][s2];
-            if (kk > gk || (kk == gk && c < j)) { gk = kk; j = c; gs = s2; }
+        // (4) the pivot: a tree over the CL headers
+        Real hk[kClusterMax];
+        int hc[kClusterMax], hs[kClusterMax];
+#pragma unroll
+        for (int s2 = 0; s2 < kClusterMax; s2++) {
+            hk[s2] = s2 < CL ? sm.hkey[par][s2] : (Real)(-1);
+            hc[s2] = s2 < CL ? sm.hcol[par][s2] : INT_MAX;
+            hs[s2] = s2;
         }
-        const T a = sm.rec[buf][gs][0];
-        if (is_zero(a) || j == INT_MAX) { dead = true; return; }
-        const T *colj = &sm.rec[buf][gs][1];
-        const bool trail_win = j >= k1;
+#pragma unroll
+        for (int w = kClusterMax / 2; w > 0; w >>= 1) {
+#pragma unroll
+            for (int s2 = 0; s2 < w; s2++) {
+                if (hk[s2 + w] > hk[s2] || (hk[s2 + w] == hk[s2] && hc[s2 + w] < hc[s2])) {
+                    hk[s2] = hk[s2 + w];
+                    hc[s2] = hc[s2 + w];
+                    hs[s2] = hs[s2 + w];
+                }
+            }
+        }
+        const int j = hc[0], gs = hs[0];
+        const T a = sm.hval[par][gs];
+        if (is_zero(a) || j == INT_MAX) { dead = true; break; }
 
-        // (5) interchange k+1 <-> j on the upper triangle
+        // (5) interchange k+1 <-> j on the upper triangle.  The trailing rows'
+        // entries come from global memory; their loads are issued here and
+        // consumed after the barriers below, so their latency overlaps them.
+        T gl[CPT];
+        bool gneg[CPT], guse[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; q++) { gl[q] = zero<T>(); gneg[q] = false; guse[q] = false; }
         if (j != k + 1) {
             const int jl = j - k0;
+            const bool trail_win = j >= k1;
             T tI = zero<T>(), tJ = zero<T>(), tRi = zero<T>(), tRj = zero<T>();
             if (!trail_win) {
-                // rows k+1 and j of every trailing column
+                // rows k+1 (position 1) and j (position jl - 2t) of every trailing column
 #pragma unroll
-                for (int q = 0; q < CPT; q++) {
-                    T ri = R[q][2 * t + 1];
-                    static_for<2 * t + 2, NB, 1>([&](auto rc) {
-                        constexpr int r = decltype(rc)::value;
-                        if (r == jl) { T tmp = R[q][r]; R[q][r] = ri; ri = tmp; }
-                    });
-                    R[q][2 * t + 1] = ri;
-                }
+                for (int q = 0; q < CPT; q++) swap_window_row<T, NB>(Rw[q], jl - 2 * t);
                 if (has_panel) {
                     const int x = tid;
                     if (x <= 2 * t) { tI = sm.lb[x][2 * t + 1]; tJ = sm.lb[x][jl]; }
@@ -390,26 +468,26 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
                 for (int q = 0; q < CPT; q++) {
                     const int c = cq[q];
                     if (c == j) {
+                        // the new column j: rows < k+1 from column k+1, (k+1, j) negated,
+                        // rows > k+1 from row k+1 negated
 #pragma unroll
-                        for (int r = 0; r < NB; r++) {
-                            if (r <= 2 * t) R[q][r] = sm.lb[r][2 * t + 1];
-                            else if (r == 2 * t + 1) R[q][r] = neg(R[q][r]);
-                            else R[q][r] = neg(sm.lb[2 * t + 1][r]);
+                        for (int p = 0; p < NB; p++) {
+                            const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
+                            if (p == 1) Rw[q][1] = neg(Rw[q][1]);
+                            else if (r <= 2 * t) Rw[q][p] = sm.lb[r][2 * t + 1];
+                            else Rw[q][p] = neg(sm.lb[2 * t + 1][r]);
                         }
                     } else if (c < n) {
-                        const T old = R[q][2 * t + 1];
-                        if (c < j) {
-                            T *p = &W[(int64_t)c * n + j];
-                            R[q][2 * t + 1] = neg(ldcg(p));
-                            stcg(p, neg(old));
-                        } else {
-                            T *p = &W[(int64_t)j * n + c];
-                            R[q][2 * t + 1] = ldcg(p);
-                            stcg(p, old);
-                        }
+                        const T old = Rw[q][1];
+                        T *pp = (c < j) ? &W[(int64_t)c * n + j] : &W[(int64_t)j * n + c];
+                        gl[q] = ldcg(pp);
+                        gneg[q] = c < j;
+                        guse[q] = true;
+                        stcg(pp, c < j ? neg(old) : old);
                     }
                 }
-                if (has_panel) tJ = colj[tid];
+                if (has_panel)
+                    tJ = ld_remote(map_rank(smem_u32(&sm.stage[par][tid]), (uint32_t)gs), (T *)nullptr);
             }
             __syncthreads();
             if (has_panel) {
@@ -427,23 +505,19 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             __syncthreads();
             parity ^= 1;
         }
+#pragma unroll
+        for (int q = 0; q < CPT; q++)
+            if (guse[q]) Rw[q][1] = gneg[q] ? neg(gl[q]) : gl[q];
 
         // (6) lazy update of row k+1, then u = row_k / a, w = -row_{k+1}
         const T ia = recip(a);
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
-            T s = R[q][2 * t + 1];
-#pragma unroll
-            for (int u = 0; u < t; u++) {
-                s = fma_(sm.lb[2 * u][2 * t + 1], R[q][2 * u + 1], s);
-                s = fms_(sm.lb[2 * u + 1][2 * t + 1], R[q][2 * u], s);
-            }
-            R[q][2 * t + 1] = neg(s);
-            R[q][2 * t] = R[q][2 * t] * ia;
+            Rw[q][1] = neg(lazy_row<T, NB>(Rw[q][1], Rw[q], sm.lb, 2 * t + 1, fin0));
+            Rw[q][0] = Rw[q][0] * ia;
         }
         if (has_panel && tid > 2 * t + 1 && pc < n) {
             T s = sm.lb[2 * t + 1][tid];
-#pragma unroll
             for (int u = 0; u < t; u++) {
                 s = fma_(sm.lb[2 * u][2 * t + 1], sm.lb[2 * u + 1][tid], s);
                 s = fms_(sm.lb[2 * u + 1][2 * t + 1], sm.lb[2 * u][tid], s);
@@ -451,8 +525,32 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             sm.lb[2 * t + 1][tid] = neg(s);
             sm.lb[2 * t][tid] = sm.lb[2 * t][tid] * ia;
         }
-        if (leader) {
-            piv[k / 2] = j;
+        if (tid == 0) {
+            sm.pivval[t] = a;
+            sm.pivcol[t] = j;
+        }
+
+        // (7) rotate the window: the finished pair goes to the end
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const T r0 = Rw[q][0], r1 = Rw[q][1];
+#pragma unroll
+            for (int p = 0; p < NB - 2; p++) Rw[q][p] = Rw[q][p + 2];
+            Rw[q][NB - 2] = r0;
+            Rw[q][NB - 1] = r1;
+        }
+        __syncthreads();
+    }
+
+    if (dead) {
+        if (leader) st->dead = 1;
+        cluster_sync();
+        return;
+    }
+    if (leader) {
+        for (int s2 = 0; s2 < t; s2++) {
+            const T a = sm.pivval[s2];
+            piv[k0 / 2 + s2] = sm.pivcol[s2];
             const double m = (double)mag(a);
             la += log(m);
             double ar, ai;
@@ -462,28 +560,26 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
             pre = nr;
             pim = ni;
         }
-        __syncthreads();
-    });
-
-    if (dead) {
-        if (leader) st->dead = 1;
-        cluster_sync();
-        return;
     }
 
-    // ---- write the factored panel rows back
+    // ---- write the factored panel rows back (t steps done: window position p
+    // holds panel row 2t+p for p < NB-2t, else row p-(NB-2t))
 #pragma unroll
     for (int q = 0; q < CPT; q++)
 #pragma unroll
-        for (int r = 0; r < NB; r++)
-            if (cq[q] < n && k0 + r < n) W[(int64_t)(k0 + r) * n + cq[q]] = R[q][r];
+        for (int p = 0; p < NB; p++) {
+            const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
+            if (cq[q] < n && k0 + r < n) W[(int64_t)(k0 + r) * n + cq[q]] = Rw[q][p];
+        }
     if (has_panel && rank == 0 && pc < n) {
         for (int r = 0; r < NB && r < tid; r++) W[(int64_t)(k0 + r) * n + pc] = sm.lb[r][tid];
     }
-    if (split.enabled) {
+    // the int8 operands of the split update; trailing columns exist only when
+    // the panel is full (t == NB/2), where the window is back in row order
+    if (split.enabled && t == NB / 2) {
 #pragma unroll
         for (int q = 0; q < CPT; q++)
-            if (cq[q] < n) split_panel_column<T, NB>(split, b, cq[q] - k1, R[q], n - k0 < NB ? n - k0 : NB);
+            if (cq[q] < n) split_panel_column<T, NB>(split, b, cq[q] - k1, Rw[q], NB);
     }
     if (leader) {
         // keep the phase on the unit circle across panels
@@ -556,17 +652,21 @@ gemm_fp64_kernel(T *__restrict__ W_all, int n, int k0, int K, const MatState *__
 #pragma unroll
             for (int jj = 0; jj < TN; jj++) acc[i][jj] = fma_(xa[i], yb[jj], acc[i][jj]);
     }
+    // per output row: all loads first, then the stores (one memory round trip per row)
 #pragma unroll
     for (int i = 0; i < TM; i++) {
         const int ar = a0 + ty + i * (BM / TM);
         if (ar >= n) continue;
+        T cv[TN];
 #pragma unroll
         for (int jj = 0; jj < TN; jj++) {
             const int bc = b0 + tx + jj * (BN / TN);
-            if (bc < n && bc > ar) {
-                T *p = &W[(int64_t)ar * n + bc];
-                *p = *p + acc[i][jj];
-            }
+            cv[jj] = (bc < n && bc > ar) ? W[(int64_t)ar * n + bc] : zero<T>();
+        }
+#pragma unroll
+        for (int jj = 0; jj < TN; jj++) {
+            const int bc = b0 + tx + jj * (BN / TN);
+            if (bc < n && bc > ar) W[(int64_t)ar * n + bc] = cv[jj] + acc[i][jj];
         }
     }
 }
