@@ -13,7 +13,7 @@
  * Matrices are batches of `batch` contiguous n x n arrays.  `layout` says how one
  * matrix is stored: PFB_ROW_MAJOR (C order, torch/NumPy default) or PFB_COL_MAJOR
  * (how XLA hands a matrix to the reference's handlers, which request
- * input_layouts=[(1, 0)] at pfcuda/cuda_api.py:57,79 and index CM(A,n,r,c) =
+ * input_layouts=[(1, 0)] at pfcuda/cuda_api.py:50,72 and index CM(A,n,r,c) =
  * A[r + c*n], include/pfaffian_utils.cuh:10).  The inputs are taken to be
  * skew-symmetric; the Pfaffian of the matrix in the stated layout is returned.
  *
@@ -74,7 +74,7 @@ int pfb_last_cuda_error(void);
  * Pf(A) for n <= 32, one value per matrix, in the input dtype.
  *
  * Replaces the XLA handlers pfaffian_f32 / _f64 / _c64 / _c128
- * (bindings/jax_bindings.cu:82-112, symbols :196-228), which launch the
+ * (bindings/jax_bindings.cu:82-112, symbols :152-183), which launch the
  * reference kernel pf_sm_calc once per matrix (src/pfaffian_sm.cu:101-105).
  * Here one launch covers the whole batch.  n == 0 or odd gives 0; n > 32 gives
  * PFB_ERR_SIZE (the reference throws, src/pfaffian.cu:44-45).  A zero pivot
@@ -89,7 +89,7 @@ int pfb_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout,
  * Replaces the XLA handlers slog_pfaffian_f32 / _f64 / _c64 / _c128
  * (bindings/jax_bindings.cu:19-80, symbols :115-150), which copy each matrix
  * and run the host-driven loop of src/slog_pfaffian_lg.cu:151-211.
- * log_out: `batch` doubles (pfcuda/cuda_api.py:78 declares the log as float64).
+ * log_out: `batch` doubles (pfcuda/cuda_api.py:71 declares the log as float64).
  * sign_out: `batch` values of `dtype`: +-1 for real input, a unit-modulus
  * phase for complex input, 0 when Pf = 0 (then log = -inf).  Odd n gives
  * (-inf, 0).  n <= 32 is accepted too (the Python layer refuses it as the

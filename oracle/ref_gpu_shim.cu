@@ -10,7 +10,7 @@
 // reference algorithm overwrites it (jax_bindings.cu:52-72).
 //
 // Each matrix is passed the way XLA hands it to the reference, column-major
-// (pfcuda/cuda_api.py:57 input_layouts=[(1, 0)]); the kernels index it with
+// (pfcuda/cuda_api.py:50 input_layouts=[(1, 0)]); the kernels index it with
 // CM(A, n, r, c) = A[r + c*n] (include/pfaffian_utils.cuh:10).
 #include <cstdint>
 #include <stdexcept>

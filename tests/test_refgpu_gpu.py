@@ -2,7 +2,7 @@
 
 oracle/_ref/libref_gpu.so is the reference's src/*.cu compiled unchanged for
 sm_100a (oracle/Makefile) with a C shim that replays its XLA handlers.  The
-reference takes each matrix column-major (pfcuda/cuda_api.py:57); the engine is
+reference takes each matrix column-major (pfcuda/cuda_api.py:50); the engine is
 called on the same buffers with PFB_COL_MAJOR.
 
 The reference differs from the engine in pivoting details -- a zero threshold of
