@@ -137,6 +137,27 @@ int pfb_slog_panel_width(int dtype, int n);
 int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
                     int32_t *piv_out, void *stream);
 
+/*
+ * pfb_slog_pfaffian without a caller workspace.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory (a plugin
+ * given raw pointers by a framework that owns all allocations, a binding with no
+ * CUDA allocator, a path where a device-synchronising cudaMalloc is not
+ * acceptable).  The scratch is one array of PFB_NOALLOC_SCRATCH_BYTES inside
+ * libpfb200.so, held on every GPU that loads the library until exit.
+ *   - Sizes whose pfb_slog_workspace_bytes(dtype, batch, n, mode) exceeds
+ *     PFB_NOALLOC_SCRATCH_BYTES return PFB_ERR_SIZE (n <= 32 needs no scratch);
+ *     e.g. one float64 matrix fits up to n = 1448 (1392 in PFB_MODE_SPLIT), one
+ *     complex128 matrix up to n = 1022 (980 in PFB_MODE_SPLIT).
+ *   - The first call on a device looks up the array's device address; make that
+ *     first call before any stream capture.
+ *   - All calls share the array: calls that overlap on the GPU race and must be
+ *     serialised by the caller.
+ * Nothing is allocated; arguments and results are those of pfb_slog_pfaffian.
+ */
+#define PFB_NOALLOC_SCRATCH_BYTES (16u << 20)
+int pfb_slog_pfaffian_noalloc(int dtype, const void *A, int64_t batch, int n, int layout,
+                              int mode, double *log_out, void *sign_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
