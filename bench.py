@@ -5,7 +5,9 @@ matrix, 2n = 4096, float64, A = (G - G^T)/2 with G ~ N(0, 1/2n) from seed 1
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
-A step is one slog_pfaffian of one matrix through the C ABI.  `value` is the
+A step is one pfb_slog_pfaffian call on a batch of independent matrices (as
+many as the GPU factors concurrently: 8 at 2n = 4096) through the C ABI; the
+batch-1 latency of each path is reported beside it.  `value` is the
 split-precision path (int8 slices on the tcgen05 tensor cores, FP64 panel) when
 it is available, else the FP64 path; the other path is timed in the same run
 and reported beside it.  Multi-GPU runs are replicas (each rank factors its own
@@ -45,6 +47,7 @@ def parse():
     p.add_argument("--n", type=int, default=N_DEFAULT)
     p.add_argument("--dtype", default="float64", choices=["float64", "complex128"])
     p.add_argument("--mode", default="auto", choices=["auto", "split", "fp64"])
+    p.add_argument("--batch", type=int, default=0, help="matrices per call (0: as many as run concurrently)")
     return p.parse_args()
 
 
@@ -174,6 +177,14 @@ def cpu_baseline(n):
 
 # ----------------------------------------------------------------- engine arm
 
+def auto_batch(n):
+    """Matrices factored concurrently per call: as many panel clusters as the
+    GPU runs at once (a cluster of ceil((n-64)/256) CTAs per matrix, at most one
+    16-CTA cluster per GPC)."""
+    cl = max(1, -(-(n - 64) // 256))
+    return max(1, min(16, 128 // max(cl, 8) if cl >= 8 else 16))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -191,21 +202,23 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
 
     n = args.n
+    B = args.batch if args.batch > 0 else auto_batch(n)
     npdt = np.float64 if args.dtype == "float64" else np.complex128
-    A_host = O.config_large(n, dtype=npdt, seed=1 + rank)[0]
+    A_host = O.config_large(n, dtype=npdt, seed=1 + rank, B=B)
     A = torch.from_numpy(A_host).to(dev)
     tdt = A.dtype
     L = _lib.lib()
     stream = torch.cuda.current_stream(dev)
+    dtc = {torch.float64: _lib.F64, torch.complex128: _lib.C128}[tdt]
+    mc = {"split": _lib.MODE_SPLIT, "fp64": _lib.MODE_FP64}
 
     def available(mode):
         try:
-            pf.slog_pfaffian_raw(A, mode=mode)
+            pf.slog_pfaffian_raw(A[:1], mode=mode)
             torch.cuda.synchronize()
             return True
         except _lib.PfbError as e:
@@ -216,17 +229,14 @@ def main():
     modes = ["split", "fp64"] if args.mode == "auto" else [args.mode]
     modes = [m for m in modes if available(m)]
     head = modes[0]
+    ws = {m: torch.empty(pf.slog_workspace_bytes(tdt, B, n, m), dtype=torch.uint8, device=dev) for m in modes}
+    la = torch.empty(B, dtype=torch.float64, device=dev)
+    sg = torch.empty(B, dtype=tdt, device=dev)
 
-    ws = {m: torch.empty(pf.slog_workspace_bytes(tdt, 1, n, m), dtype=torch.uint8, device=dev) for m in modes}
-    la = torch.empty((), dtype=torch.float64, device=dev)
-    sg = torch.empty((), dtype=tdt, device=dev)
-    dtc = {torch.float64: _lib.F64, torch.complex128: _lib.C128}[tdt]
-    mc = {"split": _lib.MODE_SPLIT, "fp64": _lib.MODE_FP64}
-
-    def step(mode, src=None):
-        st = L.pfb_slog_pfaffian(dtc, (src if src is not None else A).data_ptr(), 1, n, _lib.ROW_MAJOR,
-                                 mc[mode], la.data_ptr(), sg.data_ptr(), ws[mode].data_ptr(),
-                                 ws[mode].numel(), stream.cuda_stream)
+    def step(mode, src=None, nb=B):
+        X = src if src is not None else A
+        st = L.pfb_slog_pfaffian(dtc, X.data_ptr(), nb, n, _lib.ROW_MAJOR, mc[mode], la.data_ptr(),
+                                 sg.data_ptr(), ws[mode].data_ptr(), ws[mode].numel(), stream.cuda_stream)
         _lib.check(st, "pfb_slog_pfaffian")
 
     def barrier():
@@ -241,41 +251,43 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return t.item()
 
-    def timed(mode, k, clocks=None):
+    def timed(mode, nb, k, clocks=None):
         for _ in range(args.warmup):
-            step(mode)
+            step(mode, nb=nb)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if clocks:
             clocks.start()
         e0.record(stream)
         for _ in range(k):
-            step(mode)
+            step(mode, nb=nb)
         e1.record(stream)
         barrier()
         ck = clocks.stop() if clocks else None
         return max_over_ranks(e0.elapsed_time(e1) / k), ck
 
-    results = {}
+    results, results1 = {}, {}
     clocks = None
     for m in modes:
         cs = ClockSampler(local) if m == head else None
-        ms, ck = timed(m, args.steps, cs)
+        ms, ck = timed(m, B, args.steps, cs)
         results[m] = ms
         if ck is not None:
             clocks = ck
+        results1[m], _ = timed(m, 1, max(3, args.steps // 2))
 
-    # accuracy of the headline path against the FP64 oracle (rank 0, once)
+    # accuracy of the headline path against the FP64 oracle (rank 0)
     step(head)
     torch.cuda.synchronize()
     acc = None
     if rank == 0:
         wl, ws_ = O.slog_pf(A_host)
-        got_l, got_s = la.item(), sg.cpu().numpy()
-        acc = {"log_abs_err": abs(got_l - float(wl)), "log_rel_err": abs(got_l - float(wl)) / abs(float(wl)),
-               "sign_equal": bool(np.all(np.abs(got_s - ws_) < 1e-10))}
+        got_l, got_s = la.cpu().numpy(), sg.cpu().numpy()
+        acc = {"max_log_rel_err": float(np.max(np.abs(got_l - wl) / np.abs(wl))),
+               "max_log_abs_err": float(np.max(np.abs(got_l - wl))),
+               "sign_equal": bool(np.all(np.abs(got_s - ws_) < 1e-10)), "matrices": int(B)}
 
-    # per-kernel times of the headline path (a separate, instrumented pass)
+    # per-kernel times of the headline path (a separate, instrumented call)
     nb = L.pfb_slog_panel_width(dtc, n)
     npan = (n - 1 + nb - 1) // nb
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * npan)] for _ in range(2)]
@@ -283,10 +295,9 @@ def main():
         e.record(stream)          # creates the CUDA events (torch creates them lazily)
     torch.cuda.synchronize()
     arr = [(ctypes.c_void_p * (2 * npan))(*[e.cuda_event for e in es]) for es in evs]
-    assert all(e.cuda_event for e in evs[0] + evs[1])
     tm = _lib.SlogTiming(ctypes.cast(arr[0], ctypes.POINTER(ctypes.c_void_p)),
                          ctypes.cast(arr[1], ctypes.POINTER(ctypes.c_void_p)), npan)
-    st = L.pfb_slog_pfaffian_timed(dtc, A.data_ptr(), 1, n, _lib.ROW_MAJOR, mc[head], la.data_ptr(),
+    st = L.pfb_slog_pfaffian_timed(dtc, A.data_ptr(), B, n, _lib.ROW_MAJOR, mc[head], la.data_ptr(),
                                    sg.data_ptr(), ws[head].data_ptr(), ws[head].numel(),
                                    stream.cuda_stream, ctypes.byref(tm))
     _lib.check(st, "pfb_slog_pfaffian_timed")
@@ -294,22 +305,26 @@ def main():
     panel_ms = sum(evs[0][2 * i].elapsed_time(evs[0][2 * i + 1]) for i in range(npan))
     upd_ms = sum(evs[1][2 * i].elapsed_time(evs[1][2 * i + 1]) for i in range(npan - 1))
 
-    # end to end: pinned host input -> device -> slog -> (log, sign) back to the host
+    # end to end through the Python API: pinned host input -> device -> slog -> (log, sign) to host
     h_in = torch.from_numpy(A_host).pin_memory()
     d_in = torch.empty_like(A)
-    h_log = torch.empty((), dtype=torch.float64).pin_memory()
-    h_sign = torch.empty((), dtype=tdt).pin_memory()
-    for _ in range(args.warmup):
+    h_log = torch.empty(B, dtype=torch.float64).pin_memory()
+    h_sign = torch.empty(B, dtype=tdt).pin_memory()
+    wsh = ws[head]
+
+    def e2e_step():
         d_in.copy_(h_in, non_blocking=True)
-        step(head, d_in)
+        l2, s2 = pf.slog_pfaffian_raw(d_in, mode=head, workspace=wsh)
+        h_log.copy_(l2, non_blocking=True)
+        h_sign.copy_(s2, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        d_in.copy_(h_in, non_blocking=True)
-        step(head, d_in)
-        h_log.copy_(la, non_blocking=True)
-        h_sign.copy_(sg, non_blocking=True)
+        e2e_step()
     e1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
@@ -320,46 +335,51 @@ def main():
         return
 
     ms = results[head]
-    value = world / (ms * 1e-3)
+    value = world * B / (ms * 1e-3)
     esz = A.element_size()
-    # Roofline of the trailing update (the kernel class that carries the O(n^3)
-    # arithmetic): n^3/3 real flops (x4 complex) over its summed launch time.
-    flops = (n ** 3) / 3.0 * (4 if tdt.is_complex else 1)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    # panel: algorithmic bytes = the panel rows read and written once
-    # (2 * n^2/2 elements over all panels) -> GB/s over the summed panel time
-    panel_bytes = float(n) * n * esz
+    # trailing update, the kernel that carries the O(n^3) arithmetic: each of
+    # its launches reads and writes the upper triangle of the trailing block in
+    # FP64 once (algorithmic bytes 2 * m^2/2 * element size per matrix)
+    upd_bytes = sum(2 * (m * m / 2.0) * esz for m in (n - nb * (i + 1) for i in range(npan - 1)) if m > 0) * B
+    # panel: the panel rows are read and written once per panel
+    panel_bytes = 2.0 * (n * n / 2.0) * esz * B
     dominant = "panel" if panel_ms >= upd_ms else "update"
     if dominant == "panel":
         achieved = panel_bytes / (panel_ms * 1e-3) / 1e9
         roof = {"kernel": "panel_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "note": "latency-bound: one cluster barrier per pivot pair; bytes = panel rows read+written once"}
+                "note": "latency-bound (one cluster barrier and one global round trip per pivot pair); "
+                        "algorithmic bytes = panel rows read and written once"}
     else:
-        achieved = flops / (upd_ms * 1e-3) / 1e12
-        roof = {"kernel": "trailing update", "bound": "tensor", "achieved": achieved,
-                "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None}
+        achieved = upd_bytes / (upd_ms * 1e-3) / 1e9
+        roof = {"kernel": "split_update_kernel" if head == "split" else "gemm_fp64_kernel", "bound": "hbm",
+                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": None, "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch"}
     line = {
         "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if tdt == torch.float64 else "c128",
         "data": "synthetic",
-        "config": {"workload": f"slog_pfaffian 2n={n} {args.dtype}, seed 1 (+rank), one matrix per step",
-                   "n": n, "batch": 1, "mode": head, "panel_width": nb,
-                   "l2": f"input {n * n * esz / 1e6:.0f} MB > 126 MB L2, re-read every step",
+        "config": {"workload": f"slog_pfaffian of independent 2n={n} {args.dtype} matrices, seed 1 (+rank), "
+                               f"{B} per call", "n": n, "batch": B, "mode": head, "panel_width": nb,
+                   "l2": f"inputs {B * n * n * esz / 1e6:.0f} MB > 126 MB L2, re-read every step",
                    "parallelism": f"replicas x{world}"},
         "modes_ms_per_step": results,
-        "split_over_fp64": (results["fp64"] / results["split"]) if "split" in results and "fp64" in results else None,
+        "split_over_fp64": (results["fp64"] / results["split"]) if len(results) == 2 else None,
+        "batch1_ms": results1,
+        "batch1_matrices_per_s": {m: 1e3 / v for m, v in results1.items()},
+        "batch1_split_over_fp64": (results1["fp64"] / results1["split"]) if len(results1) == 2 else None,
         "accuracy": acc,
         "kernel_ms": {"panel": panel_ms, "update": upd_ms, "panels": npan},
         "roofline": roof,
-        "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "matrices/s",
-                "h2d_bytes_per_step": n * n * esz, "d2h_bytes_per_step": 8 + esz},
+        "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "matrices/s",
+                "h2d_bytes_per_step": B * n * n * esz, "d2h_bytes_per_step": B * (8 + esz)},
         "gpu_launches": args.steps * (2 + npan + (npan - 1)),
         "clocks": clocks,
     }
