@@ -129,6 +129,28 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
 int pfb_slog_panel_width(int dtype, int n);
 
 /*
+ * (log|Pf|, sign) of a ragged batch in one launch: `count` matrices of even (or
+ * odd) orders n[i] <= max_n <= PFB_RAGGED_MAX_N, each float32 or float64
+ * (dtype[i]), each contiguous at A[i] in `layout`.  A, n and dtype are DEVICE
+ * arrays.  log_out[i] and sign_out[i] are doubles (sign +-1, or 0 with
+ * log = -inf when Pf = 0 or the order is odd; log = NaN for an order above
+ * max_n or an unknown dtype).  Every matrix is factored in FP64.
+ *
+ * No counterpart call in the reference, whose caller loops over sizes and calls
+ * slog_pfaffian per matrix (pfcuda/cuda_api.py:57-76, each a host-driven loop,
+ * src/slog_pfaffian_lg.cu:151-211).  Nothing is allocated and the host is not
+ * synchronised, so the call may be captured in a CUDA graph and replayed.
+ * workspace: pfb_slog_ragged_workspace_bytes(count, max_n) bytes, 256-aligned.
+ */
+#define PFB_RAGGED_MAX_N 544
+int pfb_slog_pfaffian_ragged(const void *const *A, const int32_t *n, const int32_t *dtype,
+                             int64_t count, int max_n, int layout, double *log_out,
+                             double *sign_out, void *workspace, size_t workspace_bytes,
+                             void *stream);
+
+size_t pfb_slog_ragged_workspace_bytes(int64_t count, int max_n);
+
+/*
  * Pivot columns chosen by the last pfb_slog_pfaffian call that used this
  * workspace: n/2 int32 per matrix (the column index swapped into position k+1
  * at pivot step k, as the reference's argmax picks it).  Copies into the device

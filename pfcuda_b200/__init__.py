@@ -6,7 +6,7 @@ complex64 / complex128, computed by hand-written sm_100a kernels behind the C AB
 of include/pfb200.h (libpfb200.so, built in-tree).
 """
 from .api import (pfaffian, slog_pfaffian, pfaffian_raw, slog_pfaffian_raw,
-                  slog_workspace_bytes)
+                  slog_workspace_bytes, slog_pfaffian_ragged, RaggedPlan)
 
 __all__ = ["pfaffian", "slog_pfaffian", "pfaffian_raw", "slog_pfaffian_raw",
-           "slog_workspace_bytes"]
+           "slog_workspace_bytes", "slog_pfaffian_ragged", "RaggedPlan"]

@@ -147,6 +147,60 @@ def slog_pfaffian_raw(A: torch.Tensor, mode: str = "split", layout: int = _lib.R
     return la, sg
 
 
+# ------------------------------------------------------------- ragged batches
+
+class RaggedPlan:
+    """A ragged batch prepared once and run many times (one launch per run).
+
+    ``mats`` is a list of square CUDA tensors (float32 or float64, row-major
+    unless ``layout`` says otherwise) of even or odd orders up to 544.  The
+    device arrays of pointers, orders and dtypes and the workspace are built here;
+    ``run()`` enqueues the sort and the persistent factorisation kernel on the
+    current stream and returns (log|Pf|, sign) as float64 tensors.  ``run()``
+    allocates nothing, so it may be captured in a torch.cuda.CUDAGraph.
+    """
+
+    def __init__(self, mats, layout: int = _lib.ROW_MAJOR):
+        if not mats:
+            raise ValueError("empty batch")
+        dev = mats[0].device
+        for M in mats:
+            if M.ndim != 2 or M.shape[0] != M.shape[1]:
+                raise ValueError("every matrix must be square")
+            if M.dtype not in (torch.float32, torch.float64):
+                raise TypeError("ragged batches take float32 or float64 matrices")
+            if not M.is_cuda or M.device != dev:
+                raise ValueError("all matrices must be CUDA tensors on one device")
+        self.mats = [M.contiguous() for M in mats]
+        self.count = len(self.mats)
+        self.max_n = max(M.shape[0] for M in self.mats)
+        if self.max_n > 544:
+            raise ValueError("ragged batches take orders up to 544")
+        self.layout = layout
+        self.ptrs = torch.tensor([M.data_ptr() for M in self.mats], dtype=torch.int64, device=dev)
+        self.ns = torch.tensor([M.shape[0] for M in self.mats], dtype=torch.int32, device=dev)
+        self.dts = torch.tensor([_DT[M.dtype] for M in self.mats], dtype=torch.int32, device=dev)
+        wsb = int(_lib.lib().pfb_slog_ragged_workspace_bytes(self.count, self.max_n))
+        self.ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        self.log = torch.empty(self.count, dtype=torch.float64, device=dev)
+        self.sign = torch.empty(self.count, dtype=torch.float64, device=dev)
+
+    def run(self):
+        st = _lib.lib().pfb_slog_pfaffian_ragged(
+            self.ptrs.data_ptr(), self.ns.data_ptr(), self.dts.data_ptr(), self.count, self.max_n,
+            self.layout, self.log.data_ptr(), self.sign.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+            _stream(self.log))
+        _lib.check(st, "pfb_slog_pfaffian_ragged")
+        return self.log, self.sign
+
+
+def slog_pfaffian_ragged(mats, layout: int = _lib.ROW_MAJOR):
+    """(log|Pf|, sign) for a list of matrices of different orders, in one launch."""
+    plan = RaggedPlan(mats, layout)
+    la, sg = plan.run()
+    return la.clone(), sg.clone()
+
+
 # ------------------------------------------------------------- autograd glue
 
 class _PfaffianFn(torch.autograd.Function):

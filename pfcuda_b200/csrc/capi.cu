@@ -99,6 +99,27 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
     return rc;
 }
 
+size_t pfb_slog_ragged_workspace_bytes(int64_t count, int max_n)
+{
+    return pfb::ragged_workspace_bytes(count, max_n);
+}
+
+int pfb_slog_pfaffian_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, int64_t count,
+                             int max_n, int layout, double *log_out, double *sign_out, void *workspace,
+                             size_t workspace_bytes, void *stream)
+{
+    if (count < 0 || max_n < 0 || !valid_layout(layout)) return PFB_ERR_INVALID;
+    if (max_n > PFB_RAGGED_MAX_N) return PFB_ERR_SIZE;
+    if (count == 0) return PFB_OK;
+    if (!A || !n || !dtype || !log_out || !sign_out) return PFB_ERR_INVALID;
+    const size_t need = pfb::ragged_workspace_bytes(count, max_n);
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
+    const int rc = pfb::launch_ragged(A, n, dtype, count, max_n, layout, log_out, sign_out, workspace,
+                                      (cudaStream_t)stream);
+    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    return rc;
+}
+
 int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
                     int32_t *piv_out, void *stream)
 {

@@ -26,6 +26,10 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
 
 int large_panel_width(int dtype, int n);
 
+size_t ragged_workspace_bytes(int64_t count, int max_n);
+int launch_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, int64_t count, int max_n,
+                  int layout, double *log_out, double *sign_out, void *workspace, cudaStream_t s);
+
 int large_copy_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,
                       int32_t *piv_out, cudaStream_t stream);
 

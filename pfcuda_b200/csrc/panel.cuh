@@ -1,0 +1,483 @@
+// panel.cuh -- the panel factorisation of the blocked skew-LTL^T (see large.cu
+// for the whole algorithm): one cluster of CTAs (or one CTA) factors NB pivot
+// rows of one matrix, with the Gauss vectors of each trailing column in the
+// registers of one thread.
+#pragma once
+#include <limits.h>
+
+#include "common.cuh"
+#include "large.cuh"
+#include "split.cuh"
+
+namespace pfb {
+
+constexpr int kTT = 256;         // trailing-column threads per CTA
+constexpr int kClusterMax = 16;  // non-portable cluster size limit
+
+// --------------------------------------------------------------- PTX helpers
+
+PFB_D uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+PFB_D uint32_t cluster_size()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+PFB_D void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\t"
+                 "barrier.cluster.wait.acquire;" ::: "memory");
+}
+PFB_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+PFB_D uint32_t map_rank(uint32_t addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+PFB_D void st_remote(uint32_t addr, double v)
+{
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+PFB_D void st_remote(uint32_t addr, int v)
+{
+    asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+PFB_D void st_remote(uint32_t addr, c128 v)
+{
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.re), "d"(v.im) : "memory");
+}
+// L2-coherent accesses to the working matrix inside the panel kernel: other
+// CTAs of the cluster read and write the same lines between cluster barriers.
+PFB_D double ldcg(const double *p) { return __ldcg(p); }
+PFB_D c128 ldcg(const c128 *p)
+{
+    double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return mk(v.x, v.y);
+}
+PFB_D void stcg(double *p, double v) { __stcg(p, v); }
+PFB_D void stcg(c128 *p, c128 v) { __stcg(reinterpret_cast<double2 *>(p), make_double2(v.re, v.im)); }
+
+PFB_D double pkey(double x)
+{
+    double m = fabs(x);
+    return (m != m) ? INFINITY : m;
+}
+PFB_D double pkey(c128 x)
+{
+    double m = hypot(x.re, x.im);
+    return (m != m) ? INFINITY : m;
+}
+PFB_D c128 neg(c128 x) { return mk(-x.re, -x.im); }
+PFB_D double neg(double x) { return -x; }
+
+// ----------------------------------------------------------------- panel
+
+template <typename T, int NB>
+struct PanelSmem {
+    using Real = typename RealOf<T>::type;
+    static constexpr int NT = kTT;
+    static constexpr int NW = NT / 32;
+    T lb[NB][NB + 1];                  // replicated NB x NB block of the panel columns
+    alignas(16) T stage[2][NB];        // this CTA's best trailing column, panel rows 0..NB-1
+    T hval[2][kClusterMax];            // per-CTA best candidate, pushed by every CTA of the cluster
+    Real hkey[2][kClusterMax];
+    int hcol[2][kClusterMax];
+    T wval[NW];                        // per-warp best candidate
+    Real wkey[NW];
+    int wcol[NW];
+    T pivval[NB / 2];                  // this panel's pivots and pivot columns
+    int pivcol[NB / 2];
+};
+
+template <typename T> PFB_D void put(uint32_t a, T v) { st_remote(a, v); }
+PFB_D void store_pair(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
+PFB_D void store_pair(c128 *p, c128 a, c128 b) { p[0] = a; p[1] = b; }
+
+// s + sum over the window's Gauss-vector pairs (window pair index P >= fin0,
+// pair u = P - fin0) of  c_u[u] * Rw[2P+1] - c_w[u] * Rw[2P]  with
+// c_u = lb[2u][col], c_w = lb[2u+1][col].  Four partial sums shorten the
+// dependency chain; chunks of 8 pairs with a compiler barrier between them keep
+// the coefficient loads from all being hoisted into registers at once.
+template <typename T, int NB>
+PFB_D T lazy_row(T s, const T (&Rw)[NB], const T (*lb)[NB + 1], int col, int fin0)
+{
+    T s2 = zero<T>(), s3 = zero<T>(), s4 = zero<T>();
+#pragma unroll
+    for (int P0 = 0; P0 < NB / 2; P0 += 8) {
+        if (P0 + 7 >= fin0) {
+#pragma unroll
+            for (int P = P0; P < P0 + 8; P++) {
+                if (P >= 1 && P >= fin0) {
+                    const int u = P - fin0;
+                    if (P & 1) {
+                        s = fma_(lb[2 * u][col], Rw[2 * P + 1], s);
+                        s2 = fms_(lb[2 * u + 1][col], Rw[2 * P], s2);
+                    } else {
+                        s3 = fma_(lb[2 * u][col], Rw[2 * P + 1], s3);
+                        s4 = fms_(lb[2 * u + 1][col], Rw[2 * P], s4);
+                    }
+                }
+            }
+        }
+        asm volatile("" ::: "memory");
+    }
+    return (s + s2) + (s3 + s4);
+}
+
+// Interchange window rows 1 and p (2 <= p < NB, uniform across the CTA) with
+// a branch per position, so every register index stays static.
+template <typename T, int NB>
+PFB_D void swap_window_row(T (&Rw)[NB], int p)
+{
+    static_for<2, NB, 1>([&](auto pc) {
+        constexpr int P = decltype(pc)::value;
+        if (p == P) {
+            const T tmp = Rw[1];
+            Rw[1] = Rw[P];
+            Rw[P] = tmp;
+        }
+    });
+}
+
+PFB_D double ld_remote(uint32_t addr, double *)
+{
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+    return v;
+}
+PFB_D c128 ld_remote(uint32_t addr, c128 *)
+{
+    double re, im;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(re), "=d"(im) : "r"(addr) : "memory");
+    return mk(re, im);
+}
+
+// Factor panel rows [k0, k0+NB) of every matrix; one cluster of CL CTAs per
+// matrix (blockIdx.y).  Thread i of CTA rank r keeps trailing columns
+// k0+NB + r*kTT + i + q*CL*kTT (q < CPT) of the panel rows in registers; threads
+// i < NB also own panel column k0+i, whose entries live in the shared block lb.
+//
+// The register window is rotated by two rows per pivot step, so the current
+// pivot rows are always Rw[0] (row k) and Rw[1] (row k+1) and the step loop
+// stays a loop (a fully unrolled panel does not fit the instruction cache).  At
+// step t, window position p holds panel row 2t+p for p < NB-2t (rows not yet
+// factored) and panel row p-(NB-2t) otherwise (the Gauss vectors of pairs
+// 0..t-1, u_s at even and w_s at odd positions).
+//
+// A pivot step costs one cluster barrier: every CTA pushes the header of its
+// best candidate (|value|, column, value) into every CTA's shared memory before
+// it, and the owner of a CTA's best trailing column stages that column; after
+// the barrier each CTA knows the pivot, and the panel-column threads read the
+// interchanged column straight from the winning CTA's stage.
+template <typename T, int NB, int CPT>
+PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, MatState *__restrict__ st,
+                      int32_t *__restrict__ piv, const SplitArgs &split, int64_t b)
+{
+    using Real = typename RealOf<T>::type;
+    using SM = PanelSmem<T, NB>;
+    constexpr int NW = SM::NW;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const bool has_panel = tid < NB;
+    const uint32_t rank = cluster_rank();
+    const int CL = (int)cluster_size();
+
+    if (st->dead) return;   // same value for the whole cluster
+
+    const int k1 = k0 + NB;
+    const int GT = CL * kTT;
+    const int pc = k0 + tid;   // panel column of this thread (if has_panel)
+    int cq[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; q++) cq[q] = k1 + (int)rank * kTT + tid + q * GT;
+
+    // ---- load the panel rows (window position p = panel row p at step 0)
+    T Rw[CPT][NB];
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+            Rw[q][r] = (cq[q] < n && k0 + r < n) ? W[(int64_t)(k0 + r) * n + cq[q]] : zero<T>();
+    if (has_panel) {
+        for (int r = 0; r < NB; r++)
+            sm.lb[r][tid] = (k0 + r < n && pc < n) ? W[(int64_t)(k0 + r) * n + pc] : zero<T>();
+    }
+
+    double la = 0.0, pre = 1.0, pim = 0.0;
+    int parity = 0;
+    const bool leader = rank == 0 && tid == 0;
+    if (leader) {
+        la = st->log_abs;
+        pre = st->ph_re;
+        pim = st->ph_im;
+        parity = st->parity;
+    }
+    bool dead = false;
+    const int nsteps = (n - k0) / 2 < NB / 2 ? (n - k0) / 2 : NB / 2;
+    // every CTA of the cluster has started (and loaded) before any shared
+    // memory of another CTA is written
+    cluster_sync();
+
+    int t = 0;
+#pragma unroll 1
+    for (; t < nsteps; t++) {
+        const int k = k0 + 2 * t;
+        const int par = t & 1;
+        const int fin0 = NB / 2 - t;   // window pair index of the oldest Gauss-vector pair
+
+        // (1) lazy update of row k with the panel's earlier Gauss vectors
+#pragma unroll
+        for (int q = 0; q < CPT; q++) Rw[q][0] = lazy_row<T, NB>(Rw[q][0], Rw[q], sm.lb, 2 * t, fin0);
+        const bool pcand = has_panel && tid > 2 * t && pc < n;
+        T pv = zero<T>();
+        if (pcand) {
+            T s = sm.lb[2 * t][tid];
+            for (int u = 0; u < t; u++) {
+                s = fma_(sm.lb[2 * u][2 * t], sm.lb[2 * u + 1][tid], s);
+                s = fms_(sm.lb[2 * u + 1][2 * t], sm.lb[2 * u][tid], s);
+            }
+            sm.lb[2 * t][tid] = s;
+            pv = s;
+        }
+
+        // (2) this thread's best candidate (its panel column first: the
+        // smaller index), then the warp's
+        Real key = (Real)(-1);
+        int col = INT_MAX;
+        int qsel = -1;
+        T val = zero<T>();
+        if (pcand) { key = pkey(pv); col = pc; val = pv; }
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            if (cq[q] < n) {
+                Real kq = pkey(Rw[q][0]);
+                if (kq > key) { key = kq; col = cq[q]; qsel = q; val = Rw[q][0]; }
+            }
+        }
+        Real wk = key;
+        int wc = col;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            Real k2 = shfl_xor(wk, off);
+            int c2 = shfl_xor(wc, off);
+            if (k2 > wk || (k2 == wk && c2 < wc)) { wk = k2; wc = c2; }
+        }
+        if (wc != INT_MAX && col == wc) sm.wval[warp] = val;
+        if (lane == 0) { sm.wkey[warp] = wk; sm.wcol[warp] = wc; }
+        __syncthreads();
+
+        // (3) the CTA's best candidate: its header goes to every CTA of the
+        // cluster, and if it is a trailing column its owner stages the column
+        Real ck = (Real)(-1);
+        int cc = INT_MAX, cw = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            Real kk = sm.wkey[w];
+            int c = sm.wcol[w];
+            if (kk > ck || (kk == ck && c < cc)) { ck = kk; cc = c; cw = w; }
+        }
+        if (tid < CL) {
+            put(map_rank(smem_u32(&sm.hkey[par][rank]), tid), ck);
+            put(map_rank(smem_u32(&sm.hcol[par][rank]), tid), cc);
+            put(map_rank(smem_u32(&sm.hval[par][rank]), tid), sm.wval[cw]);
+        }
+        if (qsel >= 0 && col == cc) {
+#pragma unroll
+            for (int P = 0; P < NB / 2; P++) {
+                // window pair P holds panel rows (r, r+1), r even
+                const int r = (2 * P < NB - 2 * t) ? 2 * t + 2 * P : 2 * P - (NB - 2 * t);
+                T v0 = Rw[0][2 * P], v1 = Rw[0][2 * P + 1];
+#pragma unroll
+                for (int q = 1; q < CPT; q++) {
+                    v0 = (qsel == q) ? Rw[q][2 * P] : v0;
+                    v1 = (qsel == q) ? Rw[q][2 * P + 1] : v1;
+                }
+                store_pair(&sm.stage[par][r], v0, v1);
+            }
+        }
+        cluster_sync();
+
+        // (4) the pivot: a tree over the CL headers
+        Real hk[kClusterMax];
+        int hc[kClusterMax], hs[kClusterMax];
+#pragma unroll
+        for (int s2 = 0; s2 < kClusterMax; s2++) {
+            hk[s2] = s2 < CL ? sm.hkey[par][s2] : (Real)(-1);
+            hc[s2] = s2 < CL ? sm.hcol[par][s2] : INT_MAX;
+            hs[s2] = s2;
+        }
+#pragma unroll
+        for (int w = kClusterMax / 2; w > 0; w >>= 1) {
+#pragma unroll
+            for (int s2 = 0; s2 < w; s2++) {
+                if (hk[s2 + w] > hk[s2] || (hk[s2 + w] == hk[s2] && hc[s2 + w] < hc[s2])) {
+                    hk[s2] = hk[s2 + w];
+                    hc[s2] = hc[s2 + w];
+                    hs[s2] = hs[s2 + w];
+                }
+            }
+        }
+        const int j = hc[0], gs = hs[0];
+        const T a = sm.hval[par][gs];
+        if (is_zero(a) || j == INT_MAX) { dead = true; break; }
+
+        // (5) interchange k+1 <-> j on the upper triangle.  The trailing rows'
+        // entries come from global memory; their loads are issued here and
+        // consumed after the barriers below, so their latency overlaps them.
+        T gl[CPT];
+        bool gneg[CPT], guse[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; q++) { gl[q] = zero<T>(); gneg[q] = false; guse[q] = false; }
+        if (j != k + 1) {
+            const int jl = j - k0;
+            const bool trail_win = j >= k1;
+            T tI = zero<T>(), tJ = zero<T>(), tRi = zero<T>(), tRj = zero<T>();
+            if (!trail_win) {
+                // rows k+1 (position 1) and j (position jl - 2t) of every trailing column
+#pragma unroll
+                for (int q = 0; q < CPT; q++) swap_window_row<T, NB>(Rw[q], jl - 2 * t);
+                if (has_panel) {
+                    const int x = tid;
+                    if (x <= 2 * t) { tI = sm.lb[x][2 * t + 1]; tJ = sm.lb[x][jl]; }
+                    if (x > 2 * t + 1 && x < jl) { tJ = sm.lb[x][jl]; tRi = sm.lb[2 * t + 1][x]; }
+                    if (x == jl) tRi = sm.lb[2 * t + 1][jl];
+                    if (x > jl) { tRi = sm.lb[2 * t + 1][x]; tRj = sm.lb[jl][x]; }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < CPT; q++) {
+                    const int c = cq[q];
+                    if (c == j) {
+                        // the new column j: rows < k+1 from column k+1, (k+1, j) negated,
+                        // rows > k+1 from row k+1 negated
+#pragma unroll
+                        for (int p = 0; p < NB; p++) {
+                            const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
+                            if (p == 1) Rw[q][1] = neg(Rw[q][1]);
+                            else if (r <= 2 * t) Rw[q][p] = sm.lb[r][2 * t + 1];
+                            else Rw[q][p] = neg(sm.lb[2 * t + 1][r]);
+                        }
+                    } else if (c < n) {
+                        const T old = Rw[q][1];
+                        T *pp = (c < j) ? &W[(int64_t)c * n + j] : &W[(int64_t)j * n + c];
+                        gl[q] = ldcg(pp);
+                        gneg[q] = c < j;
+                        guse[q] = true;
+                        stcg(pp, c < j ? neg(old) : old);
+                    }
+                }
+                if (has_panel)
+                    tJ = ld_remote(map_rank(smem_u32(&sm.stage[par][tid]), (uint32_t)gs), (T *)nullptr);
+            }
+            __syncthreads();
+            if (has_panel) {
+                const int x = tid;
+                if (!trail_win) {
+                    if (x <= 2 * t) { sm.lb[x][2 * t + 1] = tJ; sm.lb[x][jl] = tI; }
+                    if (x > 2 * t + 1 && x < jl) { sm.lb[2 * t + 1][x] = neg(tJ); sm.lb[x][jl] = neg(tRi); }
+                    if (x == jl) sm.lb[2 * t + 1][jl] = neg(tRi);
+                    if (x > jl) { sm.lb[2 * t + 1][x] = tRj; sm.lb[jl][x] = tRi; }
+                } else {
+                    if (x <= 2 * t) sm.lb[x][2 * t + 1] = tJ;
+                    if (x > 2 * t + 1) sm.lb[2 * t + 1][x] = neg(tJ);
+                }
+            }
+            __syncthreads();
+            parity ^= 1;
+        }
+#pragma unroll
+        for (int q = 0; q < CPT; q++)
+            if (guse[q]) Rw[q][1] = gneg[q] ? neg(gl[q]) : gl[q];
+
+        // (6) lazy update of row k+1, then u = row_k / a, w = -row_{k+1}
+        const T ia = recip(a);
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            Rw[q][1] = neg(lazy_row<T, NB>(Rw[q][1], Rw[q], sm.lb, 2 * t + 1, fin0));
+            Rw[q][0] = Rw[q][0] * ia;
+        }
+        if (has_panel && tid > 2 * t + 1 && pc < n) {
+            T s = sm.lb[2 * t + 1][tid];
+            for (int u = 0; u < t; u++) {
+                s = fma_(sm.lb[2 * u][2 * t + 1], sm.lb[2 * u + 1][tid], s);
+                s = fms_(sm.lb[2 * u + 1][2 * t + 1], sm.lb[2 * u][tid], s);
+            }
+            sm.lb[2 * t + 1][tid] = neg(s);
+            sm.lb[2 * t][tid] = sm.lb[2 * t][tid] * ia;
+        }
+        if (tid == 0) {
+            sm.pivval[t] = a;
+            sm.pivcol[t] = j;
+        }
+
+        // (7) rotate the window: the finished pair goes to the end
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+            const T r0 = Rw[q][0], r1 = Rw[q][1];
+#pragma unroll
+            for (int p = 0; p < NB - 2; p++) Rw[q][p] = Rw[q][p + 2];
+            Rw[q][NB - 2] = r0;
+            Rw[q][NB - 1] = r1;
+        }
+        __syncthreads();
+    }
+
+    if (dead) {
+        if (leader) st->dead = 1;
+        cluster_sync();
+        return;
+    }
+    if (leader) {
+        for (int s2 = 0; s2 < t; s2++) {
+            const T a = sm.pivval[s2];
+            piv[k0 / 2 + s2] = sm.pivcol[s2];
+            const double m = (double)mag(a);
+            la += log(m);
+            double ar, ai;
+            if constexpr (IsComplex<T>::value) { ar = a.re / m; ai = a.im / m; }
+            else { ar = a < 0 ? -1.0 : 1.0; ai = 0.0; }
+            const double nr = pre * ar - pim * ai, ni = pre * ai + pim * ar;
+            pre = nr;
+            pim = ni;
+        }
+    }
+
+    // ---- write the factored panel rows back (t steps done: window position p
+    // holds panel row 2t+p for p < NB-2t, else row p-(NB-2t))
+#pragma unroll
+    for (int q = 0; q < CPT; q++)
+#pragma unroll
+        for (int p = 0; p < NB; p++) {
+            const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
+            if (cq[q] < n && k0 + r < n) W[(int64_t)(k0 + r) * n + cq[q]] = Rw[q][p];
+        }
+    if (has_panel && rank == 0 && pc < n) {
+        for (int r = 0; r < NB && r < tid; r++) W[(int64_t)(k0 + r) * n + pc] = sm.lb[r][tid];
+    }
+    // the int8 operands of the split update; trailing columns exist only when
+    // the panel is full (t == NB/2), where the window is back in row order
+    if (split.enabled && t == NB / 2) {
+#pragma unroll
+        for (int q = 0; q < CPT; q++)
+            if (cq[q] < n) split_panel_column<T, NB>(split, b, cq[q] - k1, Rw[q], NB);
+    }
+    if (leader) {
+        // keep the phase on the unit circle across panels
+        const double m = sqrt(pre * pre + pim * pim);
+        st->log_abs = la;
+        st->ph_re = pre / m;
+        st->ph_im = pim / m;
+        st->parity = parity;
+    }
+    cluster_sync();
+}
+
+}  // namespace pfb

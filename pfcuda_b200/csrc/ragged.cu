@@ -1,0 +1,260 @@
+// ragged.cu -- (log|Pf|, sign) of a ragged batch (matrices of different even
+// orders and of float32 or float64) in one persistent launch.
+//
+// The reference has no ragged entry point: a caller loops over sizes and calls
+// slog_pfaffian (pfcuda/cuda_api.py:57-76) once per matrix or per equal-size
+// group, and each call runs the host-driven loop of
+// src/slog_pfaffian_lg.cu:151-211.  Here one kernel covers the whole batch:
+//   * ragged_order_kernel sorts the matrix indices by order, largest first (a
+//     counting sort over n/2, one CTA), so the longest factorisations start
+//     first and the tail of the persistent loop is made of small ones;
+//   * ragged_kernel: one CTA per SM takes the next matrix from a device work
+//     counter and factors it alone: copy into its private FP64 working matrix,
+//     then for each 32-row panel the panel factorisation of large.cu run by a
+//     single CTA (panel_body with a cluster of one) followed by an in-CTA FP64
+//     skew rank-32 update of the upper trailing tiles, which stay in L2.
+// Nothing in the call synchronises the host or allocates, so a caller can
+// capture it in a CUDA graph and replay it.
+#include "common.cuh"
+#include "large.cuh"
+#include "panel.cuh"
+
+namespace pfb {
+
+constexpr int kRaggedNB = 32;        // panel width
+constexpr int kRaggedCPT = 2;        // trailing columns per thread: orders up to 32 + 2*256
+constexpr int kRaggedMaxCTAs = 160;  // workspace is sized for this many CTAs
+constexpr int kUpdTile = 64;         // in-CTA update tile (64 x 64, K = 32)
+
+struct RaggedLayout {
+    size_t order_off, counter_off, cta_off, cta_bytes, w_off, st_off, piv_off, total;
+};
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static RaggedLayout ragged_layout(int64_t count, int max_n)
+{
+    RaggedLayout L{};
+    size_t off = 0;
+    L.order_off = off;
+    off = al256(off + (size_t)count * sizeof(int32_t));
+    L.counter_off = off;
+    off = al256(off + 256);
+    L.cta_off = off;
+    L.w_off = 0;
+    L.st_off = al256((size_t)max_n * max_n * sizeof(double));
+    L.piv_off = al256(L.st_off + sizeof(MatState));
+    L.cta_bytes = al256(L.piv_off + (size_t)(max_n / 2 + 1) * sizeof(int32_t));
+    L.total = off + (size_t)kRaggedMaxCTAs * L.cta_bytes;
+    return L;
+}
+
+size_t ragged_workspace_bytes(int64_t count, int max_n)
+{
+    if (count < 0 || max_n < 0 || max_n > PFB_RAGGED_MAX_N) return 0;
+    return ragged_layout(count, max_n).total;
+}
+
+// Counting sort of the matrix indices by order, largest first (one CTA).
+__global__ void __launch_bounds__(1024)
+ragged_order_kernel(const int32_t *__restrict__ ns, int64_t count, int32_t *__restrict__ order,
+                    int *__restrict__ counter)
+{
+    constexpr int NBK = PFB_RAGGED_MAX_N / 2 + 2;
+    __shared__ int hist[NBK];
+    __shared__ int start[NBK];
+    for (int i = threadIdx.x; i < NBK; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    auto bucket = [&](int64_t i) {
+        const int n = ns[i];
+        // larger orders first; invalid orders (rejected later) go last
+        return (n < 0 || n > PFB_RAGGED_MAX_N) ? NBK - 1 : (PFB_RAGGED_MAX_N / 2 - n / 2);
+    };
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) atomicAdd(&hist[bucket(i)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < NBK; k++) { start[k] = acc; acc += hist[k]; }
+        *counter = 0;
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) {
+        const int pos = atomicAdd(&start[bucket(i)], 1);
+        order[pos] = (int32_t)i;
+    }
+}
+
+// In-CTA FP64 update of the upper trailing tiles after the panel at k0:
+// S22[a][b] += sum_r X[r][a] Y[r][b], X = panel rows, Y[2s] = X[2s+1],
+// Y[2s+1] = -X[2s].  64 x 64 tiles, 4 x 4 outputs per thread.
+PFB_D void cta_update(double *__restrict__ W, int n, int k0, int K, double (*Xs)[kUpdTile],
+                      double (*Ys)[kUpdTile])
+{
+    const int k1 = k0 + K;
+    const int m = n - k1;
+    if (m <= 0) return;
+    const int nt = (m + kUpdTile - 1) / kUpdTile;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    for (int I = 0; I < nt; I++) {
+        for (int J = I; J < nt; J++) {
+            const int a0 = k1 + I * kUpdTile, b0 = k1 + J * kUpdTile;
+            for (int e = tid; e < K * kUpdTile; e += kTT) {
+                const int r = e / kUpdTile, x = e % kUpdTile;
+                Xs[r][x] = (a0 + x < n) ? W[(int64_t)(k0 + r) * n + a0 + x] : 0.0;
+                const double y = (b0 + x < n) ? W[(int64_t)(k0 + (r ^ 1)) * n + b0 + x] : 0.0;
+                Ys[r][x] = (r & 1) ? -y : y;
+            }
+            __syncthreads();
+            double acc[4][4] = {};
+            for (int r = 0; r < K; r++) {
+                double xa[4], yb[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) xa[i] = Xs[r][ty + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; j++) yb[j] = Ys[r][tx + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[i][j] = fma(xa[i], yb[j], acc[i][j]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int ar = a0 + ty + 16 * i;
+                if (ar >= n) continue;
+                double cv[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int bc = b0 + tx + 16 * j;
+                    cv[j] = (bc < n && bc > ar) ? W[(int64_t)ar * n + bc] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int bc = b0 + tx + 16 * j;
+                    if (bc < n && bc > ar) W[(int64_t)ar * n + bc] = cv[j] + acc[i][j];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+struct RaggedSmem {
+    PanelSmem<double, kRaggedNB> panel;
+    double xs[kRaggedNB][kUpdTile];
+    double ys[kRaggedNB][kUpdTile];
+    int item;
+};
+
+__global__ void __launch_bounds__(kTT, 1)
+ragged_kernel(const void *const *__restrict__ As, const int32_t *__restrict__ ns,
+              const int32_t *__restrict__ dts, int64_t count, int max_n, int layout,
+              double *__restrict__ log_out, double *__restrict__ sign_out, unsigned char *__restrict__ ws,
+              RaggedLayout L)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RaggedSmem &sm = *reinterpret_cast<RaggedSmem *>(smem_raw);
+    const int32_t *order = reinterpret_cast<const int32_t *>(ws + L.order_off);
+    int *counter = reinterpret_cast<int *>(ws + L.counter_off);
+    unsigned char *mine = ws + L.cta_off + (size_t)blockIdx.x * L.cta_bytes;
+    double *W = reinterpret_cast<double *>(mine + L.w_off);
+    MatState *st = reinterpret_cast<MatState *>(mine + L.st_off);
+    int32_t *piv = reinterpret_cast<int32_t *>(mine + L.piv_off);
+    const int tid = threadIdx.x;
+    SplitArgs nosplit{};
+
+    for (;;) {
+        if (tid == 0) {
+            const int idx = atomicAdd(counter, 1);
+            sm.item = idx < count ? order[idx] : -1;
+        }
+        __syncthreads();
+        const int item = sm.item;
+        __syncthreads();
+        if (item < 0) break;
+        const int n = ns[item];
+        const int dt = dts[item];
+        if (n < 0 || n > max_n || (dt != PFB_F32 && dt != PFB_F64)) {
+            if (tid == 0) { log_out[item] = NAN; sign_out[item] = 0.0; }
+            continue;
+        }
+        if (n == 0 || (n & 1)) {
+            if (tid == 0) { log_out[item] = -INFINITY; sign_out[item] = 0.0; }
+            continue;
+        }
+        // copy in (the row-major view; column-major input is its transpose -A)
+        const int64_t nn = (int64_t)n * n;
+        if (dt == PFB_F64) {
+            const double *A = static_cast<const double *>(As[item]);
+            for (int64_t e = tid; e < nn; e += kTT) W[e] = A[e];
+        } else {
+            const float *A = static_cast<const float *>(As[item]);
+            for (int64_t e = tid; e < nn; e += kTT) W[e] = (double)A[e];
+        }
+        if (tid == 0) {
+            MatState s0;
+            s0.log_abs = 0.0;
+            s0.ph_re = 1.0;
+            s0.ph_im = 0.0;
+            s0.parity = 0;
+            s0.dead = 0;
+            *st = s0;
+        }
+        __syncthreads();
+        for (int k0 = 0; k0 < n - 1; k0 += kRaggedNB) {
+            panel_body<double, kRaggedNB, kRaggedCPT>(sm.panel, W, n, k0, st, piv, nosplit, 0);
+            if (st->dead) break;
+            const int K = (n - k0 < kRaggedNB) ? n - k0 : kRaggedNB;
+            cta_update(W, n, k0, K, sm.xs, sm.ys);
+            __syncthreads();
+        }
+        if (tid == 0) {
+            const MatState s = *st;
+            if (s.dead) {
+                log_out[item] = -INFINITY;
+                sign_out[item] = 0.0;
+            } else {
+                const int neg = (s.parity ^ ((layout == PFB_COL_MAJOR) ? ((n >> 1) & 1) : 0)) & 1;
+                log_out[item] = s.log_abs;
+                sign_out[item] = neg ? -s.ph_re : s.ph_re;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+int launch_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, int64_t count, int max_n,
+                  int layout, double *log_out, double *sign_out, void *workspace, cudaStream_t s)
+{
+    const RaggedLayout L = ragged_layout(count, max_n);
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    ragged_order_kernel<<<1, 1024, 0, s>>>(n, count, reinterpret_cast<int32_t *>(ws + L.order_off),
+                                          reinterpret_cast<int *>(ws + L.counter_off));
+    if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int ctas = sms < kRaggedMaxCTAs ? sms : kRaggedMaxCTAs;
+    if ((int64_t)ctas > count) ctas = (int)count;
+    const size_t smem = sizeof(RaggedSmem);
+    if (cudaFuncSetAttribute(ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return PFB_ERR_CUDA;
+    // launched as clusters of one CTA, the form the panel factorisation expects
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas, 1, 1);
+    cfg.blockDim = dim3(kTT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, ragged_kernel, A, n, dtype, count, max_n, layout, log_out, sign_out, ws, L) !=
+        cudaSuccess)
+        return PFB_ERR_CUDA;
+    return PFB_OK;
+}
+
+}  // namespace pfb
