@@ -180,6 +180,28 @@ int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspac
 int pfb_slog_pfaffian_noalloc(int dtype, const void *A, int64_t batch, int n, int layout,
                               int mode, double *log_out, void *sign_out, void *stream);
 
+/*
+ * Reverse-mode derivative of log|Pf(A)|, fused with the forward pass.
+ * Replaces the reference's differentiation rule slog_pfaffian_jvp
+ * (pfcuda/cuda_api.py:92-107), which calls jnp.linalg.inv:
+ *     d log Pf = (1/2) tr(A^-1 dA)   =>   d log Pf / dA = (1/2) A^-T
+ * (holomorphic: no conjugation; a torch or JAX wrapper conjugates as its own
+ * convention asks).  The inverse comes from the engine's own blocked skew-LTL^T
+ * factors, not from a general LU.
+ *   G_out[b] = ct_log[b] * (1/2) A[b]^-T, in the dtype and layout of A;
+ *   ct_log: batch float64 cotangents on the device, or NULL for all ones;
+ *   log_out / sign_out: the forward results, exactly as pfb_slog_pfaffian;
+ *   a matrix with Pf = 0 gets an all-NaN gradient.
+ * n must be even (odd orders have Pf = 0 identically: PFB_ERR_SIZE) and within
+ * the large path's range.  workspace: pfb_slog_grad_workspace_bytes bytes,
+ * 256-aligned (about 3 n^2 elements of the working type per matrix).
+ */
+int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                           const double *ct_log, void *G_out, double *log_out, void *sign_out,
+                           void *workspace, size_t workspace_bytes, void *stream);
+
+size_t pfb_slog_grad_workspace_bytes(int dtype, int64_t batch, int n, int mode);
+
 #ifdef __cplusplus
 }
 #endif

@@ -286,3 +286,34 @@ def tridiag_known(rng, n):
     Bq = haar_orthogonal(rng, n)
     pf = np.linalg.det(Bq) * np.prod(alt[0::2])
     return Bq @ A @ Bq.T, pf
+
+
+# ------------------------------------------------------------- derivatives
+
+def slog_pf_jvp(A, Adot):
+    """Tangent of log|Pf| by the reference's rule slog_pfaffian_jvp
+    (pfcuda/cuda_api.py:92-107): (1/2) tr(A^-1 Adot), with a general inverse
+    (NumPy's LU, standing in for jnp.linalg.inv).  Complex for complex input;
+    its real part is the derivative of log|Pf|."""
+    A = np.asarray(A)
+    Ainv = np.linalg.inv(A.astype(np.complex128 if np.iscomplexobj(A) else np.float64))
+    return 0.5 * np.einsum("...ij,...ji->...", Ainv, np.asarray(Adot))
+
+
+def slog_pf_vjp(A, ct=None):
+    """The adjoint of the same rule: ct * (1/2) A^-T per matrix (holomorphic,
+    unconjugated), so that sum(G * Adot) equals slog_pf_jvp(A, Adot) * ct."""
+    A = np.asarray(A)
+    Ainv = np.linalg.inv(A.astype(np.complex128 if np.iscomplexobj(A) else np.float64))
+    G = 0.5 * np.swapaxes(Ainv, -1, -2)
+    if ct is not None:
+        G = G * np.asarray(ct, dtype=np.float64)[..., None, None]
+    return G
+
+
+def fd_slog(A, E, h=1e-6):
+    """Central difference of log|Pf| along the direction E, (f(A+hE) - f(A-hE)) / 2h,
+    with log|Pf| from the C restatement in FP64 / C128."""
+    lp, _ = slog_pf(np.asarray(A) + h * np.asarray(E))
+    lm, _ = slog_pf(np.asarray(A) - h * np.asarray(E))
+    return (lp - lm) / (2 * h)

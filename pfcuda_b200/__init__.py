@@ -7,6 +7,8 @@ of include/pfb200.h (libpfb200.so, built in-tree).
 """
 from .api import (pfaffian, slog_pfaffian, pfaffian_raw, slog_pfaffian_raw,
                   slog_workspace_bytes, slog_pfaffian_ragged, RaggedPlan)
+from .grad import slog_pfaffian_grad, grad_workspace_bytes
 
 __all__ = ["pfaffian", "slog_pfaffian", "pfaffian_raw", "slog_pfaffian_raw",
-           "slog_workspace_bytes", "slog_pfaffian_ragged", "RaggedPlan"]
+           "slog_workspace_bytes", "slog_pfaffian_ragged", "RaggedPlan",
+           "slog_pfaffian_grad", "grad_workspace_bytes"]

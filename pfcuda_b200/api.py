@@ -213,13 +213,15 @@ class _PfaffianFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         # d Pf = (1/2) Pf tr(A^-1 dA)  (pfcuda/cuda_api.py:85-97), so
-        # dPf/dA_ij = (1/2) Pf (A^-1)_ji; torch wants conj of that for complex.
+        # dPf/dA = Pf * (1/2) A^-T, with (1/2) A^-T from the engine's adjoint
+        # kernel; torch wants the conjugate for complex A.
+        from .grad import slog_pfaffian_grad
         A, pf = ctx.saved_tensors
-        Ainv_t = torch.linalg.inv(A).transpose(-1, -2)
-        grad = 0.5 * (pf[..., None, None] * Ainv_t)
+        G = slog_pfaffian_grad(A, mode="fp64")
         if A.is_complex():
-            grad = grad.conj()
-        return g[..., None, None] * grad
+            G = G.conj()
+            pf = pf.conj()
+        return (g * pf)[..., None, None] * G
 
 
 class _SlogFn(torch.autograd.Function):
@@ -233,9 +235,10 @@ class _SlogFn(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g_log, g_sign):
+        # d log Pf = (1/2) tr(A^-1 dA)  (pfcuda/cuda_api.py:92-107); the engine
+        # returns g * (1/2) A^-T with the cotangent applied in its last kernel.
+        # torch's convention for a real function of complex A is the conjugate.
         from .grad import slog_pfaffian_grad
         (A,) = ctx.saved_tensors
-        G = slog_pfaffian_grad(A)        # d log Pf / dA = (1/2) A^-T (holomorphic)
-        if A.is_complex():
-            G = G.conj()
-        return g_log[..., None, None].to(G.dtype) * G, None
+        G = slog_pfaffian_grad(A, ct=g_log, mode=ctx.mode)
+        return (G.conj() if A.is_complex() else G), None

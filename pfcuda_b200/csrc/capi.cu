@@ -99,6 +99,31 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
     return rc;
 }
 
+size_t pfb_slog_grad_workspace_bytes(int dtype, int64_t batch, int n, int mode)
+{
+    if (!valid_dtype(dtype) || batch < 0 || n < 2 || (n & 1)) return 0;
+    return pfb::grad_workspace_bytes(dtype, batch, n, mode);
+}
+
+int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                           const double *ct_log, void *G_out, double *log_out, void *sign_out,
+                           void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
+    if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
+    if ((mode & ~0xfff) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
+    if (n < 2 || (n & 1)) return PFB_ERR_SIZE;
+    if (batch == 0) return PFB_OK;
+    if (!A || !G_out || !log_out || !sign_out) return PFB_ERR_INVALID;
+    const size_t need = pfb::grad_workspace_bytes(dtype, batch, n, mode);
+    if (need == 0) return PFB_ERR_SIZE;
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
+    const int rc = pfb::launch_grad(dtype, A, batch, n, layout, mode, ct_log, G_out, log_out, sign_out,
+                                    workspace, (cudaStream_t)stream);
+    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    return rc;
+}
+
 size_t pfb_slog_ragged_workspace_bytes(int64_t count, int max_n)
 {
     return pfb::ragged_workspace_bytes(count, max_n);

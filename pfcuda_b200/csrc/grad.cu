@@ -1,0 +1,403 @@
+// grad.cu -- the adjoint of log Pf: G = ct * d log Pf(A) / dA = ct * (1/2) A^-T,
+// formed from the engine's own factorisation.
+//
+// The reference differentiates through JAX with jax.custom_jvp rules that call
+// jnp.linalg.inv (pfcuda/cuda_api.py:78-107): d log Pf = (1/2) tr(A^-1 dA).
+// Here the inverse comes from the blocked skew-LTL^T factors of large.cu:
+//
+//   P A P^T = U^T D U,   U block-unit upper triangular (2x2 identity blocks on
+//   the diagonal), D = blockdiag(a_t J),  J = [[0, 1], [-1, 0]],
+//
+// where pair t contributes the rows U[2t] = w_t / a_t and U[2t+1] = u_t (the
+// Gauss vectors the panel kernel stores as rows 2t+1 and 2t of W), and P is the
+// product of the pivot interchanges.  Then
+//
+//   A^-1 = P^T Y D^-1 Y^T P,   Y = U^-1,   D^-1 = blockdiag(-J / a_t),
+//
+// so with Q[i][2t] = Y[i][2t+1] / a_t and Q[i][2t+1] = -Y[i][2t] / a_t,
+// (P A^-1 P^T) = Q Y^T, and G[perm[r]][perm[c]] = -(ct/2) (Q Y^T)[r][c].
+//
+// Steps (all on the device, batched over matrices):
+//   1. the forward factorisation (launch_large), which also yields (log, sign);
+//   2. grad_fix_kernel: the interchanges of later panels are applied to the
+//      Gauss vectors of earlier panels (the forward pass skips this), and the
+//      permutation perm is built;
+//   3. grad_build_u_kernel: U as an explicit n x n matrix;
+//   4. grad_diag_inv_kernel: the 64 x 64 diagonal blocks of Y = U^-1, in parallel;
+//   5. grad_block_row_kernel, block rows from the bottom: Y_I,J>I = -Y_II (U_I,>I Y_>I,J);
+//   6. grad_scatter_kernel: Q Y^T on the upper tiles, scaled and scattered to G.
+#include "common.cuh"
+#include "large.cuh"
+
+namespace pfb {
+
+constexpr int kGB = 64;   // block size of the triangular inverse and of the output tiles
+
+struct GradLayout {
+    size_t large_bytes, u_off, y_off, perm_off, total;
+};
+
+static size_t galign(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static GradLayout grad_layout(int dtype, int64_t B, int n, int mode)
+{
+    GradLayout L{};
+    const size_t ts = (dtype == PFB_C64 || dtype == PFB_C128) ? 16 : 8;
+    L.large_bytes = galign(large_workspace_bytes(dtype, B, n, mode));
+    L.u_off = L.large_bytes;
+    L.y_off = galign(L.u_off + (size_t)B * n * n * ts);
+    L.perm_off = galign(L.y_off + (size_t)B * n * n * ts);
+    L.total = galign(L.perm_off + (size_t)B * n * sizeof(int32_t));
+    return L;
+}
+
+size_t grad_workspace_bytes(int dtype, int64_t batch, int n, int mode)
+{
+    if (large_workspace_bytes(dtype, batch, n, mode) == 0) return 0;
+    return grad_layout(dtype, batch, n, mode).total;
+}
+
+// 2. interchanges of later panels applied to earlier Gauss vectors; perm
+template <typename T>
+__global__ void grad_fix_kernel(T *__restrict__ W_all, const int32_t *__restrict__ piv_all,
+                                int32_t *__restrict__ perm_all, const MatState *__restrict__ st_all, int n, int nb)
+{
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    T *W = W_all + b * (int64_t)n * n;
+    const int32_t *piv = piv_all + b * (int64_t)(n / 2);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) {
+        // row r was written by the panel starting at (r / nb) * nb; the panels
+        // after it interchanged columns it never saw
+        for (int t = ((r / nb) + 1) * nb / 2; t < n / 2; t++) {
+            const int i = 2 * t + 1, j = piv[t];
+            if (j != i) {
+                T *row = W + (int64_t)r * n;
+                const T x = row[i];
+                row[i] = row[j];
+                row[j] = x;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int32_t *perm = perm_all + b * (int64_t)n;
+        for (int q = 0; q < n; q++) perm[q] = q;
+        for (int t = 0; t < n / 2; t++) {
+            const int i = 2 * t + 1, j = piv[t];
+            const int32_t x = perm[i];
+            perm[i] = perm[j];
+            perm[j] = x;
+        }
+    }
+}
+
+// 3. U explicitly (full n x n: unit diagonal, zeros below and at (2t, 2t+1))
+template <typename T>
+__global__ void grad_build_u_kernel(const T *__restrict__ W_all, T *__restrict__ U_all,
+                                    const MatState *__restrict__ st_all, int n)
+{
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    const T *W = W_all + b * (int64_t)n * n;
+    T *U = U_all + b * (int64_t)n * n;
+    const int64_t nn = (int64_t)n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / n), c = (int)(e % n);
+        T v = zero<T>();
+        if (c == r) {
+            v = one<T>();
+        } else if (c > (r | 1)) {
+            const int t = r >> 1;
+            if (r & 1) {
+                v = W[(int64_t)(2 * t) * n + c];
+            } else {
+                const T a = W[(int64_t)(2 * t) * n + 2 * t + 1];
+                v = W[(int64_t)(2 * t + 1) * n + c] * recip(a);
+            }
+        }
+        U[e] = v;
+    }
+}
+
+// 4. Y_II = U_II^-1 for every diagonal block (zeros outside the block's upper part).
+template <typename T>
+__global__ void __launch_bounds__(kGB)
+grad_diag_inv_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all, int n)
+{
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Us = reinterpret_cast<T *>(smem_raw);          // [kGB][kGB]
+    T *Ys = Us + kGB * kGB;
+    const T *U = U_all + b * (int64_t)n * n;
+    T *Y = Y_all + b * (int64_t)n * n;
+    const int r0 = blockIdx.x * kGB;
+    const int sz = (n - r0) < kGB ? n - r0 : kGB;
+    const int j = threadIdx.x;
+    for (int i = 0; i < kGB; i++) Us[i * kGB + j] = (i < sz && j < sz) ? U[(int64_t)(r0 + i) * n + r0 + j] : zero<T>();
+    __syncthreads();
+    // column j of the inverse by back substitution, one thread per column
+    for (int i = kGB - 1; i >= 0; i--) {
+        T v = zero<T>();
+        if (i == j) {
+            v = one<T>();
+        } else if (i < j) {
+            for (int k = i + 1; k <= j; k++) v = fms_(Us[i * kGB + k], Ys[k * kGB + j], v);
+        }
+        Ys[i * kGB + j] = v;
+    }
+    for (int i = 0; i < sz; i++)
+        if (j < sz) Y[(int64_t)(r0 + i) * n + r0 + j] = Ys[i * kGB + j];
+}
+
+// 5. one block row I of Y (rows r0 .. r0+63), column tile blockIdx.x after it:
+// Y[I][c] = -Y_II * sum_{k >= r1} U[I][k] Y[k][c]
+template <typename T>
+__global__ void __launch_bounds__(256)
+grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all,
+                      int n, int r0)
+{
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Ut = reinterpret_cast<T *>(smem_raw);        // [kGB][32]
+    T *Yt = Ut + kGB * 32;                           // [32][kGB]
+    T *Ts = Yt + 32 * kGB;                           // [kGB][kGB]
+    T *Yii = Ts + kGB * kGB;                         // [kGB][kGB]
+    const T *U = U_all + b * (int64_t)n * n;
+    T *Y = Y_all + b * (int64_t)n * n;
+    const int r1 = r0 + kGB;
+    const int c0 = r1 + blockIdx.x * kGB;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
+    const int kend = (c0 + kGB < n) ? c0 + kGB : n;    // Y[k][c] = 0 for k > c
+    for (int k0 = r1; k0 < kend; k0 += 32) {
+        for (int e = tid; e < kGB * 32; e += 256) {
+            const int i = e / 32, k = e % 32;
+            Ut[e] = (r0 + i < n && k0 + k < n) ? U[(int64_t)(r0 + i) * n + k0 + k] : zero<T>();
+            const int kk = e / kGB, c = e % kGB;
+            Yt[e] = (k0 + kk < n && c0 + c < n) ? Y[(int64_t)(k0 + kk) * n + c0 + c] : zero<T>();
+        }
+        __syncthreads();
+        for (int k = 0; k < 32; k++) {
+            T ua[4], yb[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) ua[i] = Ut[(ty + 16 * i) * 32 + k];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) yb[jj] = Yt[k * kGB + tx + 16 * jj];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma_(ua[i], yb[jj], acc[i][jj]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) Ts[(ty + 16 * i) * kGB + tx + 16 * jj] = acc[i][jj];
+    for (int e = tid; e < kGB * kGB; e += 256) {
+        const int i = e / kGB, k = e % kGB;
+        Yii[e] = (r0 + i < n && r0 + k < n) ? Y[(int64_t)(r0 + i) * n + r0 + k] : zero<T>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
+    for (int k = 0; k < kGB; k++) {
+        T ya[4], tb[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) ya[i] = Yii[(ty + 16 * i) * kGB + k];
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) tb[jj] = Ts[k * kGB + tx + 16 * jj];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) acc[i][jj] = fms_(ya[i], tb[jj], acc[i][jj]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = r0 + ty + 16 * i;
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+            const int c = c0 + tx + 16 * jj;
+            if (r < n && c < n) Y[(int64_t)r * n + c] = acc[i][jj];
+        }
+    }
+}
+
+template <typename T, typename O>
+PFB_D O to_out(T v);
+template <> PFB_D double to_out<double, double>(double v) { return v; }
+template <> PFB_D float to_out<double, float>(double v) { return (float)v; }
+template <> PFB_D c128 to_out<c128, c128>(c128 v) { return v; }
+template <> PFB_D c64 to_out<c128, c64>(c128 v) { return mk((float)v.re, (float)v.im); }
+
+// 6. M = Q Y^T on the upper 64 x 64 tiles, G[perm[r]][perm[c]] = -(ct/2) M[r][c]
+// and its skew mirror.  Matrices with Pf = 0 get NaN.
+template <typename T, typename O>
+__global__ void __launch_bounds__(256)
+grad_scatter_kernel(const T *__restrict__ W_all, const T *__restrict__ Y_all, const int32_t *__restrict__ perm_all,
+                    const MatState *__restrict__ st_all, const double *__restrict__ ct, int n, O *__restrict__ G_all)
+{
+    const int64_t b = blockIdx.y;
+    O *G = G_all + b * (int64_t)n * n;
+    const int nt = (n + kGB - 1) / kGB;
+    int L = blockIdx.x, I = 0;
+    while (L >= nt - I) { L -= nt - I; I++; }
+    const int J = I + L;
+    const int i0 = I * kGB, j0 = J * kGB;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int32_t *perm = perm_all + b * (int64_t)n;
+    if (st_all[b].dead) {
+        for (int e = tid; e < kGB * kGB; e += 256) {
+            const int r = i0 + e / kGB, c = j0 + e % kGB;
+            if (r < n && c < n) {
+                T nanv;
+                if constexpr (IsComplex<T>::value) nanv = mk((double)NAN, (double)NAN);
+                else nanv = (T)NAN;
+                G[(int64_t)r * n + c] = to_out<T, O>(nanv);
+                G[(int64_t)c * n + r] = to_out<T, O>(nanv);
+            }
+        }
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LD = kGB + 1;                     // padded: the fills below walk k across lanes
+    T *Qs = reinterpret_cast<T *>(smem_raw);       // [32][LD]  Q[i][k] for the tile's rows
+    T *Ys = Qs + 32 * LD;                           // [32][LD]  Y[j][k] for the tile's columns
+    const T *W = W_all + b * (int64_t)n * n;
+    const T *Y = Y_all + b * (int64_t)n * n;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
+    for (int k0 = j0; k0 < n; k0 += 32) {            // Y[j][k] = 0 for k < j
+        for (int e = tid; e < 32 * kGB; e += 256) {
+            const int x = e >> 5, k = e & 31;        // consecutive lanes read consecutive k of a row
+            const int kg = k0 + k;
+            T q = zero<T>(), y = zero<T>();
+            if (kg < n) {
+                if (i0 + x < n) {
+                    const int t = kg >> 1;
+                    const T ia = recip(W[(int64_t)(2 * t) * n + 2 * t + 1]);
+                    q = (kg & 1) ? (-Y[(int64_t)(i0 + x) * n + 2 * t]) * ia : Y[(int64_t)(i0 + x) * n + 2 * t + 1] * ia;
+                }
+                if (j0 + x < n) y = Y[(int64_t)(j0 + x) * n + kg];
+            }
+            Qs[k * LD + x] = q;
+            Ys[k * LD + x] = y;
+        }
+        __syncthreads();
+        for (int k = 0; k < 32; k++) {
+            T qa[4], yb[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) qa[i] = Qs[k * LD + ty + 16 * i];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) yb[jj] = Ys[k * LD + tx + 16 * jj];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma_(qa[i], yb[jj], acc[i][jj]);
+        }
+        __syncthreads();
+    }
+    const double s = -0.5 * (ct ? ct[b] : 1.0);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = i0 + ty + 16 * i;
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+            const int c = j0 + tx + 16 * jj;
+            if (r < n && c < n && r <= c) {
+                const int pr = perm[r], pc = perm[c];
+                if (r == c) {
+                    G[(int64_t)pr * n + pr] = to_out<T, O>(zero<T>());
+                } else {
+                    const T g = scal(acc[i][jj], s);
+                    G[(int64_t)pr * n + pc] = to_out<T, O>(g);
+                    G[(int64_t)pc * n + pr] = to_out<T, O>(-g);
+                }
+            }
+        }
+    }
+}
+
+template <typename T>
+static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int mode, const double *ct,
+                    void *G, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s)
+{
+    const GradLayout L = grad_layout(dtype, B, n, mode);
+    int rc = launch_large(dtype, A, B, n, layout, mode, log_out, sign_out, ws, L.large_bytes, s, nullptr);
+    if (rc != PFB_OK) return rc;
+    const LargeView V = large_view(dtype, B, n, mode, ws);
+    T *W = static_cast<T *>(V.W);
+    T *U = reinterpret_cast<T *>(ws + L.u_off);
+    T *Y = reinterpret_cast<T *>(ws + L.y_off);
+    int32_t *perm = reinterpret_cast<int32_t *>(ws + L.perm_off);
+    const int nb = large_panel_width(dtype, n);
+    const unsigned ub = (unsigned)B;
+
+    grad_fix_kernel<T><<<dim3((n + 255) / 256, ub), 256, 0, s>>>(W, V.piv, perm, V.st, n, nb);
+    grad_build_u_kernel<T><<<dim3((unsigned)((int64_t)n * n / 256 + 1 < 1024 ? (int64_t)n * n / 256 + 1 : 1024), ub), 256, 0, s>>>(
+        W, U, V.st, n);
+    const int nblk = (n + kGB - 1) / kGB;
+    {
+        auto k = grad_diag_inv_kernel<T>;
+        const size_t sm = 2 * kGB * kGB * sizeof(T);
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+            return PFB_ERR_CUDA;
+        k<<<dim3((unsigned)nblk, ub), kGB, sm, s>>>(U, Y, V.st, n);
+    }
+    {
+        auto k = grad_block_row_kernel<T>;
+        const size_t sm = (2 * kGB * 32 + 2 * kGB * kGB) * sizeof(T);
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+            return PFB_ERR_CUDA;
+        for (int I = nblk - 2; I >= 0; I--) {
+            const int r0 = I * kGB;
+            const int tiles = (n - (r0 + kGB) + kGB - 1) / kGB;
+            k<<<dim3((unsigned)tiles, ub), 256, sm, s>>>(U, Y, V.st, n, r0);
+        }
+    }
+    {
+        const unsigned tiles = (unsigned)(nblk * (nblk + 1) / 2);
+        const size_t sm = 2 * 32 * (kGB + 1) * sizeof(T);
+        if (dtype == PFB_F32) {
+            auto k = grad_scatter_kernel<double, float>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<dim3(tiles, ub), 256, sm, s>>>((const double *)W, (const double *)Y, perm, V.st, ct, n, (float *)G);
+        } else if (dtype == PFB_F64) {
+            auto k = grad_scatter_kernel<double, double>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<dim3(tiles, ub), 256, sm, s>>>((const double *)W, (const double *)Y, perm, V.st, ct, n, (double *)G);
+        } else if (dtype == PFB_C64) {
+            auto k = grad_scatter_kernel<c128, c64>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<dim3(tiles, ub), 256, sm, s>>>((const c128 *)W, (const c128 *)Y, perm, V.st, ct, n, (c64 *)G);
+        } else {
+            auto k = grad_scatter_kernel<c128, c128>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<dim3(tiles, ub), 256, sm, s>>>((const c128 *)W, (const c128 *)Y, perm, V.st, ct, n, (c128 *)G);
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+}
+
+int launch_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode, const double *ct, void *G,
+                double *log_out, void *sign_out, void *workspace, cudaStream_t stream)
+{
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (dtype == PFB_C64 || dtype == PFB_C128)
+        return run_grad<c128>(dtype, A, batch, n, layout, mode, ct, G, log_out, sign_out, ws, stream);
+    return run_grad<double>(dtype, A, batch, n, layout, mode, ct, G, log_out, sign_out, ws, stream);
+}
+
+}  // namespace pfb

@@ -90,6 +90,14 @@ int large_panel_width(int dtype, int n)
     return large_cfg(dtype, n, &nb, &cpt) ? nb : 0;
 }
 
+LargeView large_view(int dtype, int64_t batch, int n, int mode, void *workspace)
+{
+    const LargeLayout L = large_layout(dtype, batch, n, mode);
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    return LargeView{reinterpret_cast<int32_t *>(ws + L.piv_off), reinterpret_cast<MatState *>(ws + L.st_off),
+                     ws + L.w_off};
+}
+
 size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode)
 {
     int nb, cpt;

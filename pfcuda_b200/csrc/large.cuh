@@ -26,6 +26,22 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
 
 int large_panel_width(int dtype, int n);
 
+// Where the factorisation leaves its results inside a large-path workspace:
+// the pivot columns (n/2 per matrix), the per-matrix state, and W, the
+// FP64 / complex128 working matrices holding the Gauss vectors (row 2t = u_t,
+// row 2t+1 = w_t right of column 2t+1, W[2t][2t+1] = the pivot a_t).
+struct LargeView {
+    int32_t *piv;
+    MatState *st;
+    void *W;
+};
+LargeView large_view(int dtype, int64_t batch, int n, int mode, void *workspace);
+
+// Declared here, defined in grad.cu: the adjoint of log|Pf|.
+size_t grad_workspace_bytes(int dtype, int64_t batch, int n, int mode);
+int launch_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode, const double *ct, void *G,
+                double *log_out, void *sign_out, void *workspace, cudaStream_t stream);
+
 size_t ragged_workspace_bytes(int64_t count, int max_n);
 int launch_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, int64_t count, int max_n,
                   int layout, double *log_out, double *sign_out, void *workspace, cudaStream_t s);

@@ -62,3 +62,22 @@ def test_workspace_sizes(dtype):
         prev = w
     assert L.pfb_slog_workspace_bytes(dtype, 2, 1024, 0) > L.pfb_slog_workspace_bytes(dtype, 1, 1024, 0)
     assert L.pfb_slog_workspace_bytes(dtype, 1, 1 << 20, 0) == 0   # beyond the supported order
+
+
+def test_grad_argument_checks_without_gpu():
+    L = _lib.lib()
+    out = ctypes.c_double()
+    p = ctypes.addressof(out)
+    f = L.pfb_slog_pfaffian_grad
+    assert f(9, p, 1, 64, 0, 0, None, p, p, p, None, 0, None) == 1      # bad dtype
+    assert f(1, p, 1, 64, 3, 0, None, p, p, p, None, 0, None) == 1      # bad layout
+    assert f(1, p, 1, 64, 0, 9, None, p, p, p, None, 0, None) == 1      # bad mode
+    assert f(1, p, 1, 35, 0, 0, None, p, p, p, None, 0, None) == 2      # odd order
+    assert f(1, p, 1, 64, 0, 0, None, p, p, p, None, 0, None) == 3      # no workspace
+    assert f(1, p, 1, 64, 0, 0, None, None, p, p, None, 0, None) == 1   # no output
+    assert f(1, p, 0, 64, 0, 0, None, p, p, p, None, 0, None) == 0      # empty batch
+    for dtype in range(4):
+        w1 = L.pfb_slog_grad_workspace_bytes(dtype, 1, 512, 0)
+        assert w1 > L.pfb_slog_workspace_bytes(dtype, 1, 512, 0) and w1 % 256 == 0
+        assert L.pfb_slog_grad_workspace_bytes(dtype, 1, 35, 0) == 0
+        assert L.pfb_slog_grad_workspace_bytes(dtype, 1, 1 << 20, 0) == 0

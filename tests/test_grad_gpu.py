@@ -1,0 +1,172 @@
+"""Adjoint of log|Pf| (pfb_slog_pfaffian_grad) against the reference's rule.
+
+The reference's slog_pfaffian_jvp (pfcuda/cuda_api.py:92-107) gives
+d log Pf = (1/2) tr(A^-1 dA); the oracle restates it with a general inverse
+(oracle.slog_pf_vjp = ct * (1/2) A^-T) and pins it against central differences
+of the C restatement of log|Pf| (h = 1e-6).
+
+Bars: relative Frobenius error <= max(1e-9, 1e-13 cond(A)) against the
+oracle's inverse for FP64 / complex128 work (both sides carry forward errors of
+order n * eps * cond(A)); <= 2e-6 for float32 / complex64 outputs (the engine
+computes in FP64 and rounds once);
+directional derivatives within 1e-6 (relative) of the central difference.
+"""
+import numpy as np
+import pytest
+import torch
+
+import pfcuda_b200 as pf
+from pfcuda_b200 import _lib
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def cuda(a):
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return np.linalg.norm((a - b).reshape(len(a), -1), axis=1) / np.linalg.norm(b.reshape(len(b), -1), axis=1)
+
+
+def bound(A):
+    """Per-matrix bar for FP64 work: max(1e-9, 1e-13 * cond_2(A))."""
+    A = np.asarray(A, dtype=np.complex128)
+    return np.maximum(1e-9, 1e-13 * np.linalg.cond(A))
+
+
+def run(A, mode="fp64", ct=None, layout=_lib.ROW_MAJOR):
+    G, la, sg = pf.slog_pfaffian_grad(cuda(A), ct=None if ct is None else cuda(ct), mode=mode,
+                                      layout=layout, return_forward=True)
+    return G.cpu().numpy(), la.cpu().numpy(), sg.cpu().numpy()
+
+
+@pytest.mark.parametrize("mode", ["fp64", "split"])
+@pytest.mark.parametrize("n", [2, 4, 8, 20, 34, 64, 66, 100, 130, 200, 290])
+def test_grad_f64(mode, n):
+    rng = np.random.default_rng(100 + n)
+    A = O.skew_normal(rng, 3, n, scale=1 / np.sqrt(n))
+    G, la, sg = run(A, mode)
+    assert G.dtype == np.float64 and G.shape == A.shape
+    assert np.all(rel(G, O.slog_pf_vjp(A)) <= bound(A))
+    assert np.allclose(G, -np.swapaxes(G, -1, -2), rtol=0, atol=0)     # exactly skew
+    wl, ws = O.slog_pf(A)
+    assert np.all(np.abs(la - wl) <= 1e-10 * np.abs(wl) + 1e-12)
+    assert np.array_equal(sg, ws)
+
+
+@pytest.mark.parametrize("mode", ["fp64", "split"])
+@pytest.mark.parametrize("n", [4, 34, 100, 256])
+def test_grad_c128(mode, n):
+    rng = np.random.default_rng(200 + n)
+    A = O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n), complex_=True)
+    G, la, sg = run(A, mode)
+    assert G.dtype == np.complex128
+    assert np.all(rel(G, O.slog_pf_vjp(A)) <= bound(A))
+    wl, ws = O.slog_pf(A)
+    assert np.all(np.abs(la - wl) <= 1e-10 * np.abs(wl) + 1e-12)
+    assert np.all(np.abs(sg - ws) <= 1e-10)
+
+
+def test_grad_workload_slice():
+    """Eight matrices of the 256 x complex128 x 512 gradient workload."""
+    A = O.config_grad()[:8]
+    ct = np.linspace(-2.0, 3.0, 8)
+    G, _, _ = run(A, "fp64", ct=ct)
+    assert np.all(rel(G, O.slog_pf_vjp(A, ct)) <= bound(A))
+
+
+@pytest.mark.parametrize("npdt", [np.float32, np.complex64])
+def test_grad_single_precision(npdt):
+    rng = np.random.default_rng(7)
+    A = O.skew_normal(rng, 2, 96, scale=0.1, complex_=np.dtype(npdt).kind == "c").astype(npdt)
+    G, _, _ = run(A)
+    assert G.dtype == npdt
+    # the engine widens the input exactly, so the oracle sees the same matrix
+    assert np.all(rel(G, O.slog_pf_vjp(A)) <= 2e-6)
+
+
+def test_grad_column_major():
+    """Memory M read column-major is A = M^T; the gradient comes back column-major."""
+    rng = np.random.default_rng(8)
+    M = O.skew_normal(rng, 2, 130, scale=1 / np.sqrt(130))
+    G, la, _ = run(M, layout=_lib.COL_MAJOR)
+    A = np.swapaxes(M, -1, -2)
+    want = np.swapaxes(O.slog_pf_vjp(A), -1, -2)     # column-major memory of the gradient
+    assert np.all(rel(G, want) <= bound(M))
+    wl, _ = O.slog_pf(A)
+    assert np.all(np.abs(la - wl) <= 1e-10 * np.abs(wl))
+
+
+def test_grad_cotangents():
+    rng = np.random.default_rng(9)
+    A = O.skew_normal(rng, 4, 66, scale=1 / np.sqrt(66))
+    G1, _, _ = run(A)
+    ct = np.array([0.5, -1.0, 0.0, 7.0])
+    Gc, _, _ = run(A, ct=ct)
+    assert np.array_equal(Gc, G1 * ct[:, None, None])      # the scale is applied in FP64 once
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_grad_matches_central_difference(cplx):
+    rng = np.random.default_rng(10 + cplx)
+    A = O.skew_normal(rng, 3, 80, scale=1 / np.sqrt(80), complex_=cplx)
+    E = O.skew_normal(rng, 3, 80, complex_=cplx)
+    G, _, _ = run(A)
+    d = np.sum(G * E, axis=(-1, -2)).real
+    fd = O.fd_slog(A, E, h=1e-6)
+    assert np.all(np.abs(d - fd) <= 1e-6 * np.abs(fd) + 1e-7), (d, fd)
+    # and against the reference's JVP rule itself
+    scale = np.sum(np.abs(O.slog_pf_vjp(A) * E), axis=(-1, -2))
+    assert np.all(np.abs(d - O.slog_pf_jvp(A, E).real) <= bound(A) * scale)
+
+
+def test_grad_zero_pfaffian_is_nan():
+    rng = np.random.default_rng(11)
+    A = O.skew_normal(rng, 2, 64, scale=0.1)
+    A[1, 5, :] = 0.0
+    A[1, :, 5] = 0.0
+    G, la, sg = run(A)
+    assert np.all(np.isfinite(G[0])) and np.all(np.isnan(G[1]))
+    assert la[1] == -np.inf and sg[1] == 0
+
+
+def test_grad_odd_order():
+    A = torch.zeros(2, 35, 35, dtype=torch.float64, device="cuda")
+    G, la, sg = pf.slog_pfaffian_grad(A, return_forward=True)
+    assert torch.isnan(G).all() and torch.isinf(la).all()
+    assert _lib.lib().pfb_slog_pfaffian_grad(_lib.F64, A.data_ptr(), 2, 35, 0, 0, None, G.data_ptr(),
+                                             la.data_ptr(), sg.data_ptr(), None, 0, None) != 0
+
+
+def test_autograd_slog_pfaffian():
+    rng = np.random.default_rng(12)
+    for cplx in (False, True):
+        A = O.skew_normal(rng, 3, 72, scale=1 / np.sqrt(72), complex_=cplx)
+        At = cuda(A).requires_grad_(True)
+        la, sg = pf.slog_pfaffian(At, mode="split")
+        w = torch.tensor([1.0, -0.5, 2.0], dtype=torch.float64, device="cuda")
+        (la * w).sum().backward()
+        want = O.slog_pf_vjp(A, w.cpu().numpy())
+        if cplx:
+            want = want.conj()
+        assert np.all(rel(At.grad.cpu().numpy(), want) <= bound(A))
+
+
+def test_autograd_pfaffian_small():
+    rng = np.random.default_rng(13)
+    for cplx in (False, True):
+        A = O.skew_normal(rng, 5, 16, complex_=cplx)
+        At = cuda(A).requires_grad_(True)
+        p = pf.pfaffian(At)
+        g = torch.ones_like(p)
+        p.backward(g)
+        pfv = O.pf_product(A)
+        want = pfv[:, None, None] * O.slog_pf_vjp(A)
+        if cplx:
+            want = want.conj()
+        assert np.all(rel(At.grad.cpu().numpy(), want) <= bound(A))

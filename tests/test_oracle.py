@@ -95,3 +95,17 @@ def test_edge_cases():
     assert np.all(np.isneginf(la)) and np.all(sg == 0)
     la, sg, piv = O.slog_pf(O.skew_normal(np.random.default_rng(1), 1, 10), with_pivots=True)
     assert piv.shape == (1, 5) and np.all(piv[0] >= np.arange(1, 10, 2))
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_jvp_rule_matches_central_difference(cplx):
+    """The restated rule of pfcuda/cuda_api.py:92-107 against central differences
+    (h = 1e-6) of the C restatement of log|Pf|, and its adjoint against the rule."""
+    rng = np.random.default_rng(20 + cplx)
+    A = O.skew_normal(rng, 3, 48, scale=1 / np.sqrt(48), complex_=cplx)
+    E = O.skew_normal(rng, 3, 48, complex_=cplx)
+    fd = O.fd_slog(A, E)
+    jvp = O.slog_pf_jvp(A, E)
+    assert np.all(np.abs(jvp.real - fd) <= 1e-6 * np.abs(fd) + 1e-7)
+    G = O.slog_pf_vjp(A, ct=[1.0, 2.0, -1.0])
+    assert np.allclose(np.sum(G * E, axis=(-1, -2)), jvp * np.array([1.0, 2.0, -1.0]), rtol=1e-12)
