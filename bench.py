@@ -48,6 +48,10 @@ def parse():
     p.add_argument("--dtype", default="float64", choices=["float64", "complex128"])
     p.add_argument("--mode", default="auto", choices=["auto", "split", "fp64"])
     p.add_argument("--batch", type=int, default=0, help="matrices per call (0: as many as run concurrently)")
+    p.add_argument("--workloads", default="all",
+                   choices=["all", "headline", "small", "ragged", "grad", "illcond"],
+                   help="'all': the headline line plus the other workloads under 'workloads'; "
+                        "a single name runs only that workload (for profiling)")
     return p.parse_args()
 
 
@@ -175,7 +179,241 @@ def cpu_baseline(n):
                       f"({dt:.1f} s)"}
 
 
+# ----------------------------------------------------------------- other workloads
+#
+# Each returns a dict that goes under "workloads" in the JSON line.  Inputs are
+# built on the host from the seeded generators, copied to the device once, and
+# every timed region brackets device work only (CUDA events on the launching
+# stream); where a workload's inputs fit in L2 (126 MB), L2 is flushed between
+# timed iterations by writing a 256 MB buffer, outside the timed events.
+
+def _ev_time(torch, stream, fn, k, warmup, flush=None):
+    """Mean device ms of fn() over k calls after warmup calls."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if flush is None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+    tot = 0.0
+    for _ in range(k):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    return tot / k
+
+
+def measure_peaks(torch, dev, stream):
+    """FP64 and INT8 tensor-core denominators measured here with library GEMMs
+    (torch.matmul float64 and torch._int_mm), for the roofline of the FP64 and
+    split updates; MEASURED_PEAKS.json carries only HBM and bf16."""
+    out = {}
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    ms = _ev_time(torch, stream, lambda: torch.matmul(a, a), 5, 2)
+    out["fp64_gemm_tflops"] = 2 * n ** 3 / (ms * 1e-3) / 1e12
+    try:
+        m = 8192
+        b = torch.randint(-64, 64, (m, m), dtype=torch.int8, device=dev)
+        ms = _ev_time(torch, stream, lambda: torch._int_mm(b, b), 5, 2)
+        out["int8_gemm_tops"] = 2 * m ** 3 / (ms * 1e-3) / 1e12
+    except RuntimeError as e:
+        out["int8_gemm_tops"] = None
+        out["int8_note"] = str(e).splitlines()[0]
+    out["how"] = "torch.matmul float64 4096^3 and torch._int_mm int8 8192^3, mean of 5 after 2 warm-up"
+    return out
+
+
+def wl_small(torch, pf, _lib, O, dev, stream, steps, warmup, hbm_peak):
+    """4096 independent 32x32 float64 matrices (seed 0): pfb_pfaffian, one launch."""
+    L = _lib.lib()
+    Ah = O.config_small()
+    A = torch.from_numpy(Ah).to(dev)
+    out = torch.empty(A.shape[0], dtype=torch.float64, device=dev)
+    B, n = A.shape[0], A.shape[-1]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def fn():
+        _lib.check(L.pfb_pfaffian(_lib.F64, A.data_ptr(), B, n, _lib.ROW_MAJOR, out.data_ptr(),
+                                  stream.cuda_stream), "pfb_pfaffian")
+
+    ms = _ev_time(torch, stream, fn, max(steps, 10), warmup, flush)
+    fn()
+    got = out.cpu().numpy()
+    want = O.pf_product(Ah, as_shipped=False)
+    rel = np.abs(got - want) / np.abs(want)
+    tri = (n * (n - 1) // 2) * 8 + 8          # strict upper triangle in, one value out
+    full = n * n * 8 + 8
+    ach_tri = B * tri / (ms * 1e-3) / 1e9
+    return {
+        "workload": "pfaffian of 4096 independent 32x32 float64 matrices, A=(G-G^T)/2, G~N(0,1), seed 0",
+        "matrices_per_s": B / (ms * 1e-3), "ms_per_call": ms, "launches_per_call": 1,
+        "l2": "256 MB written between timed calls (inputs 33.5 MB < L2)",
+        "accuracy": {"max_rel_err_vs_fp64_oracle": float(rel.max())},
+        "roofline": {"kernel": "pf_small_kernel", "bound": "hbm", "achieved": ach_tri, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": ach_tri / hbm_peak,
+                     "achieved_full_read": B * full / (ms * 1e-3) / 1e9,
+                     "note": "algorithmic bytes = strict upper triangle + result (3976 B per matrix); "
+                             "the kernel reads whole rows (8200 B), reported as achieved_full_read"},
+    }
+
+
+def wl_ragged(torch, pf, _lib, O, dev, stream, steps, warmup):
+    """2000 float32 + 2000 float64 matrices of even orders in [8, 512] (seed 2):
+    one persistent launch (captured in a CUDA graph) against a per-size loop of
+    the plain path (one batched pfb_slog_pfaffian call per (order, dtype))."""
+    cfg = O.config_ragged()
+    mats_h = cfg["float32"] + cfg["float64"]
+    mats = [torch.from_numpy(M).to(dev) for M in mats_h]
+    plan = pf.RaggedPlan(mats)
+    plan.run()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        plan.run()
+    ms_graph = _ev_time(torch, stream, g.replay, max(3, steps // 4), warmup)
+    ms_launch = _ev_time(torch, stream, plan.run, max(3, steps // 4), warmup)
+    g.replay()
+    torch.cuda.synchronize()
+    la, sg = plan.log.cpu().numpy(), plan.sign.cpu().numpy()
+
+    # per-size loop of the plain path: stacked groups, one call each
+    groups = {}
+    for i, M in enumerate(mats_h):
+        groups.setdefault((M.shape[0], M.dtype.name), []).append(i)
+    stacks = []
+    for (n, _), idx in sorted(groups.items()):
+        X = torch.stack([mats[i] for i in idx])
+        l_ = torch.empty(len(idx), dtype=torch.float64, device=dev)
+        s_ = torch.empty(len(idx), dtype=X.dtype, device=dev)
+        wsb = pf.slog_workspace_bytes(X.dtype, len(idx), n, "fp64")
+        w_ = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+        stacks.append((X, n, l_, s_, w_, wsb))
+    L = _lib.lib()
+    dmap = {torch.float32: _lib.F32, torch.float64: _lib.F64}
+
+    def loop():
+        for X, n, l_, s_, w_, wsb in stacks:
+            _lib.check(L.pfb_slog_pfaffian(dmap[X.dtype], X.data_ptr(), X.shape[0], n, _lib.ROW_MAJOR,
+                                           _lib.MODE_FP64, l_.data_ptr(), s_.data_ptr(), w_.data_ptr(),
+                                           wsb, stream.cuda_stream), "pfb_slog_pfaffian")
+
+    ms_loop = _ev_time(torch, stream, loop, max(3, steps // 4), warmup)
+    # accuracy against the FP64 oracle on every matrix (the float32 ones widened exactly)
+    wl = np.empty(len(mats_h))
+    wsg = np.empty(len(mats_h))
+    for (n, _), idx in groups.items():
+        l_, s_ = O.slog_pf(np.stack([mats_h[i].astype(np.float64) for i in idx]))
+        wl[idx], wsg[idx] = l_, s_
+    err = np.abs(la - wl) / np.maximum(np.abs(wl), 1e-300)
+    flops = sum(M.shape[0] ** 3 / 3.0 for M in mats_h)
+    cnt = len(mats_h)
+    return {
+        "workload": "ragged batch: 2000 float32 + 2000 float64 skew matrices, even orders uniform in [8, 512], "
+                    "entries N(0, 1/2n), seed 2",
+        "matrices_per_s": cnt / (ms_graph * 1e-3), "ms_per_call_graph": ms_graph,
+        "ms_per_call_direct": ms_launch, "launches_per_call": 2,
+        "per_size_loop": {"ms": ms_loop, "matrices_per_s": cnt / (ms_loop * 1e-3), "calls": len(stacks),
+                          "how": "one batched pfb_slog_pfaffian (FP64 mode) per (order, dtype) group"},
+        "speedup_vs_per_size_loop": ms_loop / ms_graph,
+        "fp64_gflops": flops / (ms_graph * 1e-3) / 1e9,
+        "accuracy": {"max_log_rel_err": float(err.max()), "sign_equal": bool(np.array_equal(sg, wsg))},
+    }
+
+
+def wl_grad(torch, pf, _lib, O, dev, stream, steps, warmup):
+    """256 complex128 matrices of order 512 (seed 3), loss = sum log|Pf|:
+    forward + adjoint in one pfb_slog_pfaffian_grad call."""
+    Ah = O.config_grad()
+    A = torch.from_numpy(Ah).to(dev)
+    B, n = A.shape[0], A.shape[-1]
+    res = {"workload": "VJP of sum log|Pf| over 256 complex128 matrices of order 512, A=(G-G^T)/2, "
+                       "Re/Im N(0, 1/2n), seed 3"}
+    ct = torch.ones(B, dtype=torch.float64, device=dev)
+    for mode in ("fp64", "split"):
+        ws = torch.empty(pf.grad_workspace_bytes(A.dtype, B, n, mode), dtype=torch.uint8, device=dev)
+
+        def fn():
+            pf.slog_pfaffian_grad(A, ct, mode=mode, workspace=ws)
+
+        ms = _ev_time(torch, stream, fn, max(3, steps // 2), warmup)
+        wsf = torch.empty(pf.slog_workspace_bytes(A.dtype, B, n, mode), dtype=torch.uint8, device=dev)
+        msf = _ev_time(torch, stream, lambda: pf.slog_pfaffian_raw(A, mode, workspace=wsf),
+                       max(3, steps // 2), warmup)
+        res[mode] = {"matrices_per_s": B / (ms * 1e-3), "ms_per_call": ms, "forward_only_ms": msf}
+    G = pf.slog_pfaffian_grad(A[:8], mode="split").cpu().numpy()
+    want = O.slog_pf_vjp(Ah[:8])
+    rel = np.linalg.norm((G - want).reshape(8, -1), axis=1) / np.linalg.norm(want.reshape(8, -1), axis=1)
+    rng = np.random.default_rng(33)
+    E = O.skew_normal(rng, 2, n, complex_=True)
+    d = np.sum(G[:2] * E, axis=(-1, -2)).real
+    fd = O.fd_slog(Ah[:2], E, h=1e-6)
+    jvp = O.slog_pf_jvp(Ah[:2], E).real
+    ms_inv = _ev_time(torch, stream, lambda: torch.linalg.inv(A), 3, 1)
+    res.update({
+        "accuracy": {"max_rel_frobenius_err_vs_half_inv_T": float(rel.max()),
+                     "max_rel_err_vs_central_difference_h1e-6": float(np.max(np.abs(d - fd) / np.abs(fd))),
+                     "max_rel_err_vs_reference_jvp_rule": float(np.max(np.abs(d - jvp) / np.abs(jvp))),
+                     "checked": "8 matrices vs (1/2) inv(A)^T; 2 directional derivatives vs FD and the JVP rule"},
+        "torch_linalg_inv_ms": ms_inv,
+        "note": "torch_linalg_inv_ms is the general inverse alone (the reference's rule calls jnp.linalg.inv)",
+    })
+    return res
+
+
+def wl_illcond(torch, pf, _lib, O, dev, stream, steps, warmup):
+    """64 float32 and 64 float64 matrices of order 2048, A = Q blockdiag(s_k J) Q^T,
+    s_k log-spaced in [1e-6, 1] (seed 4): split-precision forward and VJP error
+    against the exact log|Pf| and the FP64 oracle."""
+    Ah, exact_log, exact_sign = O.config_illcond()
+    B, n = Ah.shape[0], Ah.shape[-1]
+    res = {"workload": "ill-conditioned: 64 float32 and 64 float64 matrices, 2n=2048, "
+                       "A = Q blockdiag(s_k J) Q^T, Q Haar, s_k logspace(-6, 0), seed 4"}
+    for name, npdt in (("float64", np.float64), ("float32", np.float32)):
+        A = torch.from_numpy(Ah.astype(npdt)).to(dev)
+        ws = torch.empty(pf.slog_workspace_bytes(A.dtype, B, n, "split"), dtype=torch.uint8, device=dev)
+        ms = _ev_time(torch, stream, lambda: pf.slog_pfaffian_raw(A, "split", workspace=ws),
+                      max(2, steps // 4), min(warmup, 2))
+        la, sg = pf.slog_pfaffian_raw(A, "split", workspace=ws)
+        la, sg = la.cpu().numpy(), sg.cpu().numpy()
+        sub = 4
+        wl, wsg = O.slog_pf(Ah[:sub].astype(npdt).astype(np.float64))
+        r = {"matrices_per_s": B / (ms * 1e-3), "ms_per_call": ms,
+             "max_log_rel_err_vs_exact": float(np.max(np.abs(la - exact_log) / np.abs(exact_log))),
+             "sign_equal_exact": bool(np.array_equal(np.sign(sg), exact_sign)),
+             "max_log_rel_err_vs_fp64_oracle": float(np.max(np.abs(la[:sub] - wl) / np.abs(wl))),
+             "oracle_matrices": sub}
+        G = pf.slog_pfaffian_grad(A[:2], mode="split").cpu().numpy().astype(np.float64)
+        want = O.slog_pf_vjp(Ah[:2].astype(npdt).astype(np.float64))
+        r["vjp_max_rel_frobenius_err"] = float(np.max(
+            np.linalg.norm((G - want).reshape(2, -1), axis=1) / np.linalg.norm(want.reshape(2, -1), axis=1)))
+        res[name] = r
+        del A, ws
+        torch.cuda.empty_cache()
+    res["note"] = ("float32 inputs are rounded from the float64 matrices, so their exact-value error "
+                   "includes that rounding (cond ~ 1e6); the oracle column uses the rounded matrix")
+    return res
+
+
 # ----------------------------------------------------------------- engine arm
+
+def _hbm_peak():
+    """Measured copy bandwidth of this GPU type (MEASURED_PEAKS.json), else the
+    pool's earlier measurement."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
 
 def auto_batch(n):
     """Matrices factored concurrently per call: as many panel clusters as the
@@ -204,6 +442,20 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
+
+    stream0 = torch.cuda.current_stream(dev)
+    single = {"small": wl_small, "ragged": wl_ragged, "grad": wl_grad, "illcond": wl_illcond}
+    if args.workloads in single:
+        kw = dict(torch=torch, pf=pf, _lib=_lib, O=O, dev=dev, stream=stream0, steps=args.steps,
+                  warmup=args.warmup)
+        if args.workloads == "small":
+            kw["hbm_peak"] = _hbm_peak()
+        r = single[args.workloads](**kw)
+        if rank == 0:
+            print(json.dumps({"workloads": {args.workloads: r}}))
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     n = args.n
     B = args.batch if args.batch > 0 else auto_batch(n)
@@ -337,12 +589,7 @@ def main():
     ms = results[head]
     value = world * B / (ms * 1e-3)
     esz = A.element_size()
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_peak = _hbm_peak()
     # trailing update, the kernel that carries the O(n^3) arithmetic: each of
     # its launches reads and writes the upper triangle of the trailing block in
     # FP64 once (algorithmic bytes 2 * m^2/2 * element size per matrix)
@@ -385,6 +632,22 @@ def main():
     }
     if world == 1:
         line["cpu_baseline"] = cpu_baseline(n)
+    if world == 1 and args.workloads == "all":
+        # the other configurations, on the same GPU after the headline
+        del A, ws, d_in
+        torch.cuda.empty_cache()
+        kw = dict(torch=torch, pf=pf, _lib=_lib, O=O, dev=dev, stream=stream, steps=args.steps,
+                  warmup=args.warmup)
+        line["peaks_measured_here"] = measure_peaks(torch, dev, stream)
+        wls = {}
+        for name, fn in (("small", wl_small), ("ragged", wl_ragged), ("grad", wl_grad),
+                         ("illcond", wl_illcond)):
+            t0 = time.perf_counter()
+            extra = {"hbm_peak": hbm_peak} if name == "small" else {}
+            wls[name] = fn(**kw, **extra)
+            wls[name]["wall_s"] = time.perf_counter() - t0
+            torch.cuda.empty_cache()
+        line["workloads"] = wls
     print(json.dumps(line))
     if pg is not None:
         pg.destroy_process_group()
