@@ -130,19 +130,36 @@ PFB_D T lazy_row(T s, const T (&Rw)[NB], const T (*lb)[NB + 1], int col, int fin
     return (s + s2) + (s3 + s4);
 }
 
-// Interchange window rows 1 and p (2 <= p < NB, uniform across the CTA) with
-// a branch per position, so every register index stays static.
+// The same lazy update for a panel column c (its entries live in lb): row r
+// gains sum_{u<t} lb[2u][r] lb[2u+1][c] - lb[2u+1][r] lb[2u][c], in four
+// partial sums.
 template <typename T, int NB>
-PFB_D void swap_window_row(T (&Rw)[NB], int p)
+PFB_D T lazy_panel(const T (*lb)[NB + 1], T s, int r, int c, int t)
 {
-    static_for<2, NB, 1>([&](auto pc) {
-        constexpr int P = decltype(pc)::value;
-        if (p == P) {
-            const T tmp = Rw[1];
-            Rw[1] = Rw[P];
-            Rw[P] = tmp;
-        }
-    });
+    T s2 = zero<T>(), s3 = zero<T>(), s4 = zero<T>();
+    int u = 0;
+    for (; u + 1 < t; u += 2) {
+        s = fma_(lb[2 * u][r], lb[2 * u + 1][c], s);
+        s2 = fms_(lb[2 * u + 1][r], lb[2 * u][c], s2);
+        s3 = fma_(lb[2 * u + 2][r], lb[2 * u + 3][c], s3);
+        s4 = fms_(lb[2 * u + 3][r], lb[2 * u + 2][c], s4);
+    }
+    if (u < t) {
+        s = fma_(lb[2 * u][r], lb[2 * u + 1][c], s);
+        s2 = fms_(lb[2 * u + 1][r], lb[2 * u][c], s2);
+    }
+    return (s + s2) + (s3 + s4);
+}
+
+// Window row p (2 <= p < NB, uniform across the CTA) by a chain of selects,
+// so every register index stays static.
+template <typename T, int NB>
+PFB_D T window_row(const T (&Rw)[NB], int p)
+{
+    T v = Rw[1];
+#pragma unroll
+    for (int i = 2; i < NB; i++) v = (i == p) ? Rw[i] : v;
+    return v;
 }
 
 PFB_D double ld_remote(uint32_t addr, double *)
@@ -239,11 +256,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         const bool pcand = has_panel && tid > 2 * t && pc < n;
         T pv = zero<T>();
         if (pcand) {
-            T s = sm.lb[2 * t][tid];
-            for (int u = 0; u < t; u++) {
-                s = fma_(sm.lb[2 * u][2 * t], sm.lb[2 * u + 1][tid], s);
-                s = fms_(sm.lb[2 * u + 1][2 * t], sm.lb[2 * u][tid], s);
-            }
+            const T s = lazy_panel<T, NB>(sm.lb, sm.lb[2 * t][tid], 2 * t, tid, t);
             sm.lb[2 * t][tid] = s;
             pv = s;
         }
@@ -305,27 +318,19 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         }
         cluster_sync();
 
-        // (4) the pivot: a tree over the CL headers
-        Real hk[kClusterMax];
-        int hc[kClusterMax], hs[kClusterMax];
+        // (4) the pivot: a butterfly over the CL <= 16 headers, lane s of every
+        // warp reading header s (registers stay free for the window)
+        Real hk = lane < CL ? sm.hkey[par][lane] : (Real)(-1);
+        int hc = lane < CL ? sm.hcol[par][lane] : INT_MAX;
+        int hs = lane;
 #pragma unroll
-        for (int s2 = 0; s2 < kClusterMax; s2++) {
-            hk[s2] = s2 < CL ? sm.hkey[par][s2] : (Real)(-1);
-            hc[s2] = s2 < CL ? sm.hcol[par][s2] : INT_MAX;
-            hs[s2] = s2;
+        for (int off = kClusterMax / 2; off > 0; off >>= 1) {
+            const Real k2 = shfl_xor(hk, off);
+            const int c2 = shfl_xor(hc, off);
+            const int s2 = shfl_xor(hs, off);
+            if (k2 > hk || (k2 == hk && c2 < hc)) { hk = k2; hc = c2; hs = s2; }
         }
-#pragma unroll
-        for (int w = kClusterMax / 2; w > 0; w >>= 1) {
-#pragma unroll
-            for (int s2 = 0; s2 < w; s2++) {
-                if (hk[s2 + w] > hk[s2] || (hk[s2 + w] == hk[s2] && hc[s2 + w] < hc[s2])) {
-                    hk[s2] = hk[s2 + w];
-                    hc[s2] = hc[s2 + w];
-                    hs[s2] = hs[s2 + w];
-                }
-            }
-        }
-        const int j = hc[0], gs = hs[0];
+        const int j = shfl(hc, 0), gs = shfl(hs, 0);
         const T a = sm.hval[par][gs];
         if (is_zero(a) || j == INT_MAX) { dead = true; break; }
 
@@ -334,16 +339,25 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         // consumed after the barriers below, so their latency overlaps them.
         T gl[CPT];
         bool gneg[CPT], guse[CPT];
+        // an interchange inside the panel: window position qswap takes the old
+        // row k+1 (r1s) in the rotation at the end of the step
+        T r1s[CPT];
+        int qswap = -1;
 #pragma unroll
-        for (int q = 0; q < CPT; q++) { gl[q] = zero<T>(); gneg[q] = false; guse[q] = false; }
+        for (int q = 0; q < CPT; q++) { gl[q] = zero<T>(); gneg[q] = false; guse[q] = false; r1s[q] = zero<T>(); }
         if (j != k + 1) {
             const int jl = j - k0;
             const bool trail_win = j >= k1;
             T tI = zero<T>(), tJ = zero<T>(), tRi = zero<T>(), tRj = zero<T>();
             if (!trail_win) {
-                // rows k+1 (position 1) and j (position jl - 2t) of every trailing column
+                // rows k+1 (position 1) and j (position jl - 2t) of every
+                // trailing column: row j moves up now, row k+1 down in (7)
+                qswap = jl - 2 * t;
 #pragma unroll
-                for (int q = 0; q < CPT; q++) swap_window_row<T, NB>(Rw[q], jl - 2 * t);
+                for (int q = 0; q < CPT; q++) {
+                    r1s[q] = Rw[q][1];
+                    Rw[q][1] = window_row<T, NB>(Rw[q], qswap);
+                }
                 if (has_panel) {
                     const int x = tid;
                     if (x <= 2 * t) { tI = sm.lb[x][2 * t + 1]; tJ = sm.lb[x][jl]; }
@@ -405,11 +419,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
             Rw[q][0] = Rw[q][0] * ia;
         }
         if (has_panel && tid > 2 * t + 1 && pc < n) {
-            T s = sm.lb[2 * t + 1][tid];
-            for (int u = 0; u < t; u++) {
-                s = fma_(sm.lb[2 * u][2 * t + 1], sm.lb[2 * u + 1][tid], s);
-                s = fms_(sm.lb[2 * u + 1][2 * t + 1], sm.lb[2 * u][tid], s);
-            }
+            const T s = lazy_panel<T, NB>(sm.lb, sm.lb[2 * t + 1][tid], 2 * t + 1, tid, t);
             sm.lb[2 * t + 1][tid] = neg(s);
             sm.lb[2 * t][tid] = sm.lb[2 * t][tid] * ia;
         }
@@ -418,12 +428,13 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
             sm.pivcol[t] = j;
         }
 
-        // (7) rotate the window: the finished pair goes to the end
+        // (7) rotate the window: the finished pair goes to the end, and the old
+        // row k+1 lands where row j was
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             const T r0 = Rw[q][0], r1 = Rw[q][1];
 #pragma unroll
-            for (int p = 0; p < NB - 2; p++) Rw[q][p] = Rw[q][p + 2];
+            for (int p = 0; p < NB - 2; p++) Rw[q][p] = (p + 2 == qswap) ? r1s[q] : Rw[q][p + 2];
             Rw[q][NB - 2] = r0;
             Rw[q][NB - 1] = r1;
         }

@@ -53,8 +53,14 @@ template <> struct PhaseAcc<float> { using type = double; };
 
 // One group of G lanes per matrix.  OUT_SLOG selects (log|Pf|, sign) output
 // instead of the plain product.
+//
+// The pivot-step loop is a rolled loop over k: each lane's registers hold a
+// window of its column, window position p = row k+p at step k, and the Schur
+// update of row k+2+p writes window position p, so the window advances by two
+// rows per step without extra moves and every register index is static.  (A
+// fully unrolled elimination overflows the instruction cache at G = 32.)
 template <typename T, int G, bool OUT_SLOG>
-__global__ void __launch_bounds__(kSmallThreads)
+__global__ void __launch_bounds__(kSmallThreads, (sizeof(T) * G <= 256) ? 2 : 1)
 pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
                 T *__restrict__ out_val, double *__restrict__ out_log, T *__restrict__ out_sign)
 {
@@ -71,6 +77,7 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
     const int grp = lane / G;
     T *X = &s_x[warp][grp * G];
     T *Y = &s_y[warp][grp * G];
+    const unsigned gmask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
 
     const int64_t nn = (int64_t)n * n;
     const int64_t total_warps = (int64_t)gridDim.x * kSmallWarps;
@@ -92,12 +99,10 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
         double la = 0.0;
         Ph ph = one<Ph>();
 
-        static_for<0, G - 1, 2>([&](auto kc) {
-            constexpr int k = decltype(kc)::value;
-            if (k >= n - 1) return;     // uniform: n is the same for the whole launch
-
+#pragma unroll 1
+        for (int k = 0; k < n - 1; k += 2) {
             // ---- pivot: first maximum of |A[k][c]| over logical columns c > k
-            Real key = (lbl > k && lbl < n) ? pivot_key(R[k]) : (Real)(-1);
+            Real key = (lbl > k && lbl < n) ? pivot_key(R[0]) : (Real)(-1);
             int col = lbl;
 #pragma unroll
             for (int off = G / 2; off > 0; off >>= 1) {
@@ -107,19 +112,19 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
             }
             const int j = col;
             const unsigned ball = __ballot_sync(0xffffffffu, lbl == j);
-            const unsigned gmask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
             const int src = __ffs((ball >> (grp * G)) & gmask) - 1;
-            const T a = shfl(R[k], src, G);
+            const T a = shfl(R[0], src, G);
             dead = dead || is_zero(a);
 
-            // ---- interchange k+1 <-> j: rows by register select, columns by relabel
+            // ---- interchange k+1 <-> j: columns by relabel; rows inside the
+            // update below (window position q = j - k takes the old row k+1,
+            // row k+1 becomes the old row j)
+            const int q = j - k;
+            const T r1 = R[1];
+            T rq = r1;
+#pragma unroll
+            for (int p = 2; p < G; p++) rq = (p == q) ? R[p] : rq;
             if (!dead && j != k + 1) {
-                T ri = R[k + 1];
-                static_for<k + 2, G, 1>([&](auto rc) {
-                    constexpr int r = decltype(rc)::value;
-                    if (r == j) { T t = R[r]; R[r] = ri; ri = t; }
-                });
-                R[k + 1] = ri;
                 lbl = (lbl == k + 1) ? j : ((lbl == j) ? k + 1 : lbl);
                 swaps ^= 1;
             }
@@ -132,25 +137,30 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
                 }
             }
 
-            // ---- rank-2 Schur update S[r][c] -= (x_r y_c - y_r x_c) / a
-            X[lbl] = R[k];
-            Y[lbl] = R[k + 1];
+            // ---- rank-2 Schur update S[r][c] -= (x_r y_c - y_r x_c) / a, row
+            // k+2+p into window position p
+            X[lbl] = R[0];
+            Y[lbl] = rq;
             __syncwarp();
             if (!dead && lbl > k + 1 && lbl < n) {
                 const T ia = recip(a);
-                const T xh = R[k] * ia;
-                const T yh = R[k + 1] * ia;
-                static_for<k + 2, G, 1>([&](auto rc) {
-                    constexpr int r = decltype(rc)::value;
-                    if (r < n) {
-                        const T xr = X[r];
-                        const T yr = Y[r];
-                        R[r] = fma_(yr, xh, fms_(xr, yh, R[r]));
+                const T xh = R[0] * ia;
+                const T yh = rq * ia;
+                // chunks of 4 rows: the compiler barrier keeps it from hoisting
+                // every shared-memory load of the step (register pressure)
+#pragma unroll
+                for (int p0 = 0; p0 < G - 2; p0 += 4) {
+#pragma unroll
+                    for (int p = p0; p < p0 + 4 && p < G - 2; p++) {
+                        const int r = k + 2 + p;
+                        const T old = (p + 2 == q) ? r1 : R[p + 2];
+                        if (r < n) R[p] = fma_(Y[r], xh, fms_(X[r], yh, old));
                     }
-                });
+                    asm volatile("" ::: "memory");
+                }
             }
             __syncwarp();
-        });
+        }
 
         if (valid && gl == 0) {
             const bool neg = (swaps ^ (flip & (n >> 1))) & 1;
@@ -182,7 +192,7 @@ static int launch_small_t(const void *A, int64_t batch, int n, int layout, void 
     const int64_t mpw = 32 / G;
     const int64_t warps = (batch + mpw - 1) / mpw;
     int64_t blocks = (warps + kSmallWarps - 1) / kSmallWarps;
-    const int64_t cap = (int64_t)sms * 8;   // grid-stride beyond ~8 blocks per SM
+    const int64_t cap = (int64_t)sms * 16;   // grid-stride beyond 16 blocks per SM
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     const int flip = layout == PFB_COL_MAJOR ? 1 : 0;

@@ -30,7 +30,10 @@
 // of TN columns; the epilogue warps read their TMEM lanes back with tcgen05.ld.
 // Every mbarrier wait is bounded; a wait that gives up marks the matrix in
 // SplitArgs::err and the kernel frees its TMEM and returns.
+#include <cuda.h>
 #include <stdio.h>
+
+#include <mutex>
 
 #include "split.cuh"
 #include "large.cuh"
@@ -188,44 +191,110 @@ struct TileWalk {
     }
 };
 
+// ------------------------------------------------- tensor-map (TMA) helpers
+
+PFB_D void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];"
+                 ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
+}
+PFB_D void tma_store_3d(const CUtensorMap *map, int x, int y, int z, uint32_t src)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+                 ::"l"(map), "r"(x), "r"(y), "r"(z), "r"(src) : "memory");
+}
+PFB_D void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+PFB_D void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+PFB_D void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+PFB_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+PFB_D void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+// AND of p over the 256 epilogue threads (a barrier all of them reach), so that
+// a timed-out wait ends the loop of every epilogue thread together
+PFB_D bool epi_all(bool p)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred pi, po;\n\t"
+                 "setp.ne.u32 pi, %1, 0;\n\t"
+                 "bar.red.and.pred po, 1, 256, pi;\n\t"
+                 "selp.u32 %0, 1, 0, po;\n\t}"
+                 : "=r"(r) : "r"((uint32_t)p) : "memory");
+    return r != 0;
+}
+
+// 2^e as a double: built from its bits in the normal range, else by scalbn
+// (subnormal and overflowing powers).
+PFB_D double exp2i(int e)
+{
+    if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
+    return scalbn(1.0, e);
+}
+
+// sum_l P_l 2^(7(6-l)) for the S <= 7 digit levels of one output (|P_l| < 2^23):
+// adjacent levels pair up exactly in int32 (P_l * 2^7 + P_(l+1) < 2^31), the
+// first FP64 step is exact (< 2^46), the last two round.  The rounding is far
+// below the splitting's own truncation (K * 2^-49 relative).
+PFB_D double fold_levels(const int32_t (&P)[kSplitMaxSlices])
+{
+    const int32_t q01 = P[0] * 128 + P[1];
+    const int32_t q23 = P[2] * 128 + P[3];
+    const int32_t q45 = P[4] * 128 + P[5];
+    double t = fma((double)q01, 0x1p14, (double)q23);
+    t = fma(t, 0x1p14, (double)q45);
+    return fma(t, 0x1p7, (double)P[6]);
+}
+
+// The C tile (128 rows x 64 doubles) moves as 4 boxes of 16 doubles x 128 rows
+// with the 128-byte swizzle: double d of row r sits at byte
+//   (d / 16) * 16384 + r * 128 + (((d % 16) / 2) ^ (r % 8)) * 16 + (d % 2) * 8,
+// so the epilogue's row-per-thread 16-byte accesses are free of bank conflicts.
+constexpr int kCBoxCols = 16;
+constexpr int kCBoxBytes = kCBoxCols * kSplitTileM * 8;    // 16 KB
+constexpr int kCTileBytes = 4 * kCBoxBytes;                // 64 KB
+PFB_D uint32_t cswz(int r, int d)
+{
+    return (uint32_t)((d >> 4) * kCBoxBytes + r * 128 + ((((d & 15) >> 1) ^ (r & 7)) << 4));
+}
+
 // Persistent, warp-specialised update of the upper-triangle (128 x TN) tiles
 // of one matrix's trailing block (blockIdx.y = matrix, blockIdx.x = CTA):
-//   warp 0   bulk copies of the operand chunks (the TMA engine),
+//   warp 0   bulk copies of the int8 operand chunks,
 //   warp 1   one thread issues the tcgen05 MMAs,
 //   warps 2-9  epilogue: warp w reads TMEM lane quarter w%4 (the only one it
 //            may access) and the half h = (w-2)/4 of the tile's columns.
-// Each CTA walks a contiguous range of tiles, so consecutive tiles mostly share
-// the A operand (the 128 trailing rows), which stays in shared memory; the B
-// operands rotate through two stages.  The S digit-level accumulators of a tile
-// (NOUT * S * TN <= 448 TMEM columns) are handed back to the MMA thread as soon
-// as the epilogue has read them, so the next tile's MMAs overlap this tile's
-// FP64 read-modify-write of W, and the C values of the next tile are loaded
-// while its MMAs run.
+// The FP64 tile of W (C) travels by TMA in both directions: one epilogue
+// thread loads the tile after next into one of two shared buffers while the
+// current one is updated in place, then stores it back with a bulk tensor store
+// (out-of-range rows and columns are zero-filled on load and clipped on store;
+// the whole tile is written, including the part below the diagonal of diagonal
+// tiles, which the factorisation never reads).  Each CTA walks a contiguous
+// range of tiles, so consecutive tiles mostly share the A operand (the 128
+// trailing rows), which stays in shared memory.  The S digit-level accumulators
+// of a tile (NOUT * S * TN <= 448 TMEM columns) are handed back to the MMA
+// thread as soon as the epilogue has read them, so the next tile's MMAs overlap
+// this tile's FP64 read-modify-write.
 //
-// Epilogue arithmetic: |P_l| < 2^23 (at most 7 * 64 products of 127^2), so
-//   hi = sum_{l<=3} P_l * 2^(7(3-l)),  lo = sum_{l>=4} P_l * 2^(7(6-l))
-// are exact integers below 2^53, and the tile value is
-//   2^(e_a+e_b) * (hi * 2^-35 + lo * 2^-56)
-// with a single rounding.
+// Epilogue arithmetic: the tile value is 2^(e_a+e_b-56) * sum_l P_l 2^(7(6-l))
+// (fold_levels), added to C with one fused multiply-add.
 template <int TN, int NOUT>
 __global__ void __launch_bounds__(kSplitThreads, 1)
-split_update_kernel(void *__restrict__ W_all, int n, int k0, int K, MatState *__restrict__ st_all,
-                    SplitArgs sa)
+split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int K,
+                    MatState *__restrict__ st_all, SplitArgs sa)
 {
     constexpr int TM = kSplitTileM;
     constexpr uint32_t TMEM_COLS = 512;
-    constexpr int CW = TN / 2;                  // columns per epilogue thread
-    constexpr int NV = CW * NOUT / 2;           // double2 vectors of W per thread and tile
+    constexpr int CW = TN / 2;                  // logical columns per epilogue thread
+    static_assert(TN * NOUT == 64, "a C tile is 64 doubles wide");
     extern __shared__ __align__(1024) unsigned char smem[];
     const int kk = sa.kk;
     const int S = sa.slices;
     const int a_bytes = TM * kk;                // one slice of the A tile
     const int b_bytes = TN * kk;                // one slice of one B tile
-    const int bstage = NOUT * kSplitMaxSlices * b_bytes;
-    unsigned char *sA = smem;
-    unsigned char *sB = sA + kSplitMaxSlices * a_bytes;     // two stages
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + 2 * bstage);
-    // bars: 0 a_full, 1 a_empty, 2-3 b_full, 4-5 b_empty, 6 acc_full, 7 acc_empty
+    unsigned char *sC = smem;                                   // 2 x 64 KB, 1024-aligned
+    unsigned char *sA = sC + 2 * kCTileBytes;
+    unsigned char *sB = sA + kSplitMaxSlices * a_bytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + NOUT * kSplitMaxSlices * b_bytes);
+    // bars: 0 a_full, 1 a_empty, 2 b_full, 3 b_empty, 4 acc_full, 5 acc_empty, 6-7 c_full
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
     int *s_fail = reinterpret_cast<int *>(tmem_slot + 1);
 
@@ -244,12 +313,12 @@ split_update_kernel(void *__restrict__ W_all, int n, int k0, int K, MatState *__
     const int ntiles = t1 - t0;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    uint32_t bar[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) bar[i] = su32(&bars[i]);
+    // mbarrier i sits at bar0 + 8 i (an address, not an array: a runtime index
+    // into a register array would move it to local memory)
+    const uint32_t bar0 = su32(bars);
+    auto mb = [bar0](int i) { return bar0 + 8u * (uint32_t)i; };
     if (tid == 0) {
-        for (int i = 0; i < 7; i++) mbar_init(bar[i], 1);
-        mbar_init(bar[7], 256);
+        for (int i = 0; i < 8; i++) mbar_init(mb(i), i == 5 ? 256u : 1u);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *s_fail = 0;
     }
@@ -263,9 +332,12 @@ split_update_kernel(void *__restrict__ W_all, int n, int k0, int K, MatState *__
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
+    // copies in flight, for the drain on a failure: A loads issued, B loads
+    // issued (producer), C loads issued and consumed (epilogue leader)
+    int p_aloads = 0, p_bloads = 0, c_issued = 0, c_done = 0, m_issued = 0;
 
     if (warp == 0) {
-        // ---------------- producer
+        // ---------------- producer of the int8 operands
         if (lane == 0) {
             const int64_t chunk = (int64_t)TM * kk;
             TileWalk tw{ntn, R, 0, 0};
@@ -273,29 +345,29 @@ split_update_kernel(void *__restrict__ W_all, int n, int k0, int K, MatState *__
             int arow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, tw.next()) {
                 if (tw.I != arow) {
-                    if (aloads > 0) ok = mbar_wait_bounded(bar[1], (aloads - 1) & 1);
+                    if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1);
                     if (!ok) break;
-                    mbar_expect_tx(bar[0], (uint32_t)(S * a_bytes));
+                    mbar_expect_tx(mb(0), (uint32_t)(S * a_bytes));
                     for (int s = 0; s < S; s++)
                         bulk_g2s(su32(sA + s * a_bytes),
-                                 sa.xs + b * sa.mstride + ((int64_t)s * sa.ntile + tw.I) * chunk, a_bytes, bar[0]);
+                                 sa.xs + b * sa.mstride + ((int64_t)s * sa.ntile + tw.I) * chunk, a_bytes, mb(0));
                     arow = tw.I;
                     aloads++;
+                    p_aloads = aloads;
                 }
-                const int st = it & 1;
-                if (it >= 2) ok = mbar_wait_bounded(bar[4 + st], ((it >> 1) - 1) & 1);
+                if (it >= 1) ok = mbar_wait_bounded(mb(3), (it - 1) & 1);
                 if (!ok) break;
                 const int jrow = tw.J * TN;
                 const int64_t boff = (int64_t)(jrow / TM) * chunk + (int64_t)((jrow % TM) >> 3) * (kk >> 4) * 128;
-                mbar_expect_tx(bar[2 + st], (uint32_t)(S * NOUT * b_bytes));
-                unsigned char *dst = sB + st * bstage;
+                mbar_expect_tx(mb(2), (uint32_t)(S * NOUT * b_bytes));
                 for (int s = 0; s < S; s++) {
-                    bulk_g2s(su32(dst + s * b_bytes), sa.ys + b * sa.mstride + (int64_t)s * sa.ntile * chunk + boff,
-                             b_bytes, bar[2 + st]);
+                    bulk_g2s(su32(sB + s * b_bytes), sa.ys + b * sa.mstride + (int64_t)s * sa.ntile * chunk + boff,
+                             b_bytes, mb(2));
                     if (NOUT == 2)
-                        bulk_g2s(su32(dst + (kSplitMaxSlices + s) * b_bytes),
-                                 sa.ys2 + b * sa.mstride + (int64_t)s * sa.ntile * chunk + boff, b_bytes, bar[2 + st]);
+                        bulk_g2s(su32(sB + (kSplitMaxSlices + s) * b_bytes),
+                                 sa.ys2 + b * sa.mstride + (int64_t)s * sa.ntile * chunk + boff, b_bytes, mb(2));
                 }
+                p_bloads = it + 1;
             }
             if (!ok) atomicExch(s_fail, 1);
         }
@@ -312,141 +384,204 @@ split_update_kernel(void *__restrict__ W_all, int n, int k0, int K, MatState *__
             int arow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, tw.next()) {
                 if (tw.I != arow) {
-                    if (aloads > 0) mma_commit(bar[1]);          // A may be replaced once these MMAs finish
-                    ok = mbar_wait_bounded(bar[0], aloads & 1);
+                    if (aloads > 0) mma_commit(mb(1));          // A may be replaced once these MMAs finish
+                    ok = mbar_wait_bounded(mb(0), aloads & 1);
                     if (!ok) break;
                     arow = tw.I;
                     aloads++;
                 }
-                const int st = it & 1;
-                ok = mbar_wait_bounded(bar[2 + st], (it >> 1) & 1);
-                if (ok && it >= 1) ok = mbar_wait_bounded(bar[7], (it - 1) & 1);
+                ok = mbar_wait_bounded(mb(2), it & 1);
+                if (ok && it >= 1) ok = mbar_wait_bounded(mb(5), (it - 1) & 1);
                 if (!ok) break;
                 tc_fence_after();
-                const uint64_t bst = bdesc0 + (uint64_t)((st * bstage) >> 4);
                 for (int o = 0; o < NOUT; o++) {
                     for (int l = 0; l < S; l++) {
                         const uint32_t dcol = (uint32_t)((o * S + l) * TN);
                         for (int i = 0; i <= l; i++) {
                             const uint64_t ad = adesc0 + (uint64_t)((i * a_bytes) >> 4);
-                            const uint64_t bd = bst + (uint64_t)(((o * kSplitMaxSlices + (l - i)) * b_bytes) >> 4);
+                            const uint64_t bd = bdesc0 + (uint64_t)(((o * kSplitMaxSlices + (l - i)) * b_bytes) >> 4);
                             for (int kc = 0; kc < kk / 32; kc++)
                                 mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
                                        (i > 0 || kc > 0) ? 1u : 0u);
                         }
                     }
                 }
-                mma_commit(bar[4 + st]);     // B stage free once these MMAs are done
-                mma_commit(bar[6]);          // accumulators ready
+                mma_commit(mb(3));          // B free once these MMAs are done
+                mma_commit(mb(4));          // accumulators ready
+                m_issued = it + 1;
             }
             if (!ok) atomicExch(s_fail, 1);
         }
     } else {
         // ---------------- epilogue (warps 2-9), thread = tile row
+        const bool leader = tid == 64;
         const int quarter = warp & 3;
         const int h = (warp - 2) >> 2;
-        const int lane_row = quarter * 32 + lane;
-        double *Wd = reinterpret_cast<double *>(W_all) + (int64_t)NOUT * b * (int64_t)n * n;
+        const int r = quarter * 32 + lane;          // row within the tile
+        const int bz = (int)b;
         TileWalk tw{ntn, R, 0, 0};
         tw.start(t0);
-        double2 cv[NV];
-        auto load_c = [&](const TileWalk &w) {
-            const int arow = k1 + w.I * TM + lane_row;
-            const int bc0 = k1 + w.J * TN + h * CW;
-            const double2 *src = reinterpret_cast<const double2 *>(Wd + NOUT * ((int64_t)arow * n + bc0));
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                const int bcol = bc0 + (2 * v) / NOUT;
-                const bool any = arow < n && bcol < n && (bcol + (NOUT == 1 ? 1 : 0)) > arow;
-                cv[v] = any ? src[v] : make_double2(0.0, 0.0);
-            }
-        };
-        load_c(tw);
+        TileWalk tl = tw;                           // the leader's load cursor, one tile ahead
+        // (tile coordinates are passed by value: a reference would put the
+        // cursors in local memory)
+#define PFB_LOAD_C(buf, I_, J_)                                                                          \
+    do {                                                                                                \
+        c_issued++;                                                                                     \
+        mbar_expect_tx(mb(6 + (buf)), (uint32_t)kCTileBytes);                                          \
+        const int y_ = k1 + (I_) * TM, x0_ = NOUT * (k1 + (J_) * TN);                                   \
+        _Pragma("unroll") for (int q = 0; q < 4; q++)                                                   \
+            tma_load_3d(su32(sC + (buf) * kCTileBytes + q * kCBoxBytes), &cmap, x0_ + q * kCBoxCols, y_, bz, \
+                        mb(6 + (buf)));                                                                \
+    } while (0)
+        if (leader) {
+            PFB_LOAD_C(0, tl.I, tl.J);
+            tl.next();
+            if (ntiles > 1) PFB_LOAD_C(1, tl.I, tl.J);
+        }
         for (int it = 0; it < ntiles && ok; it++) {
-            ok = mbar_wait_bounded(bar[6], it & 1);
-            if (!ok) break;
-            tc_fence_after();
-            const int arow = k1 + tw.I * TM + lane_row;
+            const int buf = it & 1;
+            // this tile's scale exponents, loaded before the waits: the row's
+            // own, and lane c's the one of column c of this thread's half
+            const int arow = k1 + tw.I * TM + r;
             const int bc0 = k1 + tw.J * TN + h * CW;
             const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
-            double *dst = Wd + NOUT * ((int64_t)arow * n + bc0);
-            // 8 columns at a time: the S levels folded exactly into hi / lo
+            const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
+            if (leader && it >= 1 && it + 1 < ntiles) {
+                // the store of tile it-1 has read its buffer: load tile it+1 there
+                bulk_wait_read0();
+                tl.next();
+                PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
+            }
+            bool w_ok = mbar_wait_bounded(mb(6 + buf), (it >> 1) & 1);
+            if (w_ok) c_done = it + 1;
+            if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1);
+            ok = epi_all(w_ok);
+            if (!ok) break;
+            tc_fence_after();
+            unsigned char *cb = sC + buf * kCTileBytes;
+            // 8 logical columns at a time
 #pragma unroll
             for (int c8 = 0; c8 < CW / 8; c8++) {
                 double dv[NOUT][8];
 #pragma unroll
                 for (int o = 0; o < NOUT; o++) {
-                    long long hi[8], lo[8];
+                    int32_t v[kSplitMaxSlices][8];
 #pragma unroll
-                    for (int c = 0; c < 8; c++) { hi[c] = 0; lo[c] = 0; }
+                    for (int l = 0; l < kSplitMaxSlices; l++)
+                        if (l < S)
+                            tmem_ld8(tmem + ((uint32_t)(quarter * 32) << 16) +
+                                         (uint32_t)((o * S + l) * TN + h * CW + c8 * 8), v[l]);
+                    tmem_ld_wait();
 #pragma unroll
-                    for (int l0 = 0; l0 < kSplitMaxSlices; l0 += 2) {
-                        int32_t v[2][8];
+                    for (int c = 0; c < 8; c++) {
+                        int32_t P[kSplitMaxSlices];
 #pragma unroll
-                        for (int li = 0; li < 2; li++)
-                            if (l0 + li < S)
-                                tmem_ld8(tmem + ((uint32_t)(quarter * 32) << 16) +
-                                             (uint32_t)((o * S + l0 + li) * TN + h * CW + c8 * 8), v[li]);
-                        tmem_ld_wait();
-#pragma unroll
-                        for (int li = 0; li < 2; li++) {
-                            const int l = l0 + li;
-                            if (l < S) {
-#pragma unroll
-                                for (int c = 0; c < 8; c++) {
-                                    if (l <= 3) hi[c] += (long long)v[li][c] << (7 * (3 - l));
-                                    else lo[c] += (long long)v[li][c] << (7 * (6 - l));
-                                }
-                            }
-                        }
+                        for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l][c] : 0;
+                        dv[o][c] = fold_levels(P);
                     }
-#pragma unroll
-                    for (int c = 0; c < 8; c++) dv[o][c] = fma((double)lo[c], 0x1p-56, (double)hi[c] * 0x1p-35);
                 }
                 if (c8 == CW / 8 - 1) {
                     // every TMEM read of this tile is done: the MMA thread may go on
                     tc_fence_before();
-                    mbar_arrive(bar[7]);
+                    mbar_arrive(mb(5));
                 }
-                if (arow < n) {
+                // read-modify-write of the 8 * NOUT doubles in shared memory:
+                // C += value * 2^(ea + eb - 56), one rounding
+                double sc[8];
 #pragma unroll
-                    for (int c = 0; c < 8; c++) {
-                        const int col = c8 * 8 + c, bcol = bc0 + col;
-                        if (bcol < n && bcol > arow) {
-                            const int e = ea + __ldg(&sa.ex[b * n + bcol]);
+                for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
+                const int d0 = h * 32 + c8 * 8 * NOUT;
 #pragma unroll
-                            for (int o = 0; o < NOUT; o++) {
-                                const int idx = NOUT * col + o;        // position in the row segment
-                                const double old = (idx & 1) ? cv[idx >> 1].y : cv[idx >> 1].x;
-                                dst[idx] = old + scalbn(dv[o][c], e);
-                            }
-                        }
+                for (int pr = 0; pr < 4 * NOUT; pr++) {
+                    double2 *pp = reinterpret_cast<double2 *>(cb + cswz(r, d0 + 2 * pr));
+                    double2 old = *pp;
+                    if (NOUT == 1) {
+                        old.x = fma(dv[0][2 * pr], sc[2 * pr], old.x);
+                        old.y = fma(dv[0][2 * pr + 1], sc[2 * pr + 1], old.y);
+                    } else {
+                        old.x = fma(dv[0][pr], sc[pr], old.x);
+                        old.y = fma(dv[NOUT - 1][pr], sc[pr], old.y);
                     }
+                    *pp = old;
                 }
             }
+            // the tile in shared memory is complete: one thread stores it
+            fence_proxy_async();
+            epi_sync();
+            if (leader) {
+                const int y = k1 + tw.I * TM, x0 = NOUT * (k1 + tw.J * TN);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    tma_store_3d(&cmap, x0 + q * kCBoxCols, y, bz, su32(cb + q * kCBoxBytes));
+                bulk_commit();
+            }
             tw.next();
-            if (it + 1 < ntiles) load_c(tw);
         }
+#undef PFB_LOAD_C
+        if (leader) bulk_wait0();
         if (!ok) atomicExch(s_fail, 1);
     }
 
     tc_fence_before();
     __syncthreads();
-    if (tid == 0 && *s_fail) atomicExch(&sa.err[b], PFB_ERR_TIMEOUT);
+    if (*s_fail) {
+        // a wait gave up: let this CTA's copies in flight land (bounded) before exit
+        if (tid == 0) {
+            if (p_aloads > 0) mbar_wait_bounded(mb(0), (p_aloads - 1) & 1);
+            if (p_bloads > 0) mbar_wait_bounded(mb(2), (p_bloads - 1) & 1);
+            atomicExch(&sa.err[b], PFB_ERR_TIMEOUT);
+        }
+        if (tid == 32 && m_issued > 0) mbar_wait_bounded(mb(4), (m_issued - 1) & 1);   // MMAs done
+        if (tid == 64)
+            for (int t = c_done; t < c_issued; t++) mbar_wait_bounded(mb(6 + (t & 1)), (t >> 1) & 1);
+        __syncthreads();
+    }
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
-// At least 116 KB, so that a single CTA (which holds all 512 TMEM columns)
-// is resident per SM and no allocation ever waits for another CTA.
 template <int TN, int NOUT>
 static size_t split_smem_bytes(int kk)
 {
-    const size_t need = (size_t)kSplitMaxSlices * kSplitTileM * kk + 2 * (size_t)NOUT * kSplitMaxSlices * TN * kk +
-                        8 * 8 + 16;
-    return need < 116 * 1024 ? 116 * 1024 : need;
+    return (size_t)2 * kCTileBytes + (size_t)kSplitMaxSlices * kSplitTileM * kk +
+           (size_t)NOUT * kSplitMaxSlices * TN * kk + 8 * 8 + 16;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// W of a batch as a 3-D FP64 tensor {NOUT*n columns, n rows, batch}, boxes of
+// 16 doubles x 128 rows with the 128-byte swizzle.
+static bool make_c_map(CUtensorMap *map, void *W, int n, int nout, int64_t batch)
+{
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nout * n, (cuuint64_t)n, (cuuint64_t)batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)nout * n * 8, (cuuint64_t)nout * n * n * 8};
+    const cuuint32_t box[3] = {(cuuint32_t)kCBoxCols, (cuuint32_t)kSplitTileM, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, W, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int TN, int NOUT>
@@ -465,11 +600,13 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     int per = (int)(sms / batch);
     if (per > (tiles + 1) / 2) per = (tiles + 1) / 2;
     if (per < 1) per = 1;
+    CUtensorMap map;
+    if (!make_c_map(&map, W, n, NOUT, batch)) return PFB_ERR_UNSUPPORTED;
     auto k = split_update_kernel<TN, NOUT>;
     const size_t smem = split_smem_bytes<TN, NOUT>(sa.kk);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PFB_ERR_CUDA;
-    k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(W, n, k0, K, st, sa);
+    k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(map, n, k0, K, st, sa);
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
