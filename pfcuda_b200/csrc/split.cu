@@ -276,7 +276,12 @@ PFB_D uint32_t cswz(int r, int d)
 //
 // Epilogue arithmetic: the tile value is 2^(e_a+e_b-56) * sum_l P_l 2^(7(6-l))
 // (fold_levels), added to C with one fused multiply-add.
-template <int TN, int NOUT>
+//
+// KK (the K of the int8 products) and S (digit slices) are template
+// parameters: with them the MMA issue loop unrolls into constant descriptor
+// offsets.  (A loop with run-time bounds issued one MMA per ~130 cycles on
+// B200, against ~54 unrolled: the issue, not the tensor pipe, was the limit.)
+template <int TN, int NOUT, int KK, int S>
 __global__ void __launch_bounds__(kSplitThreads, 1)
 split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int K,
                     MatState *__restrict__ st_all, SplitArgs sa)
@@ -285,11 +290,11 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     constexpr uint32_t TMEM_COLS = 512;
     constexpr int CW = TN / 2;                  // logical columns per epilogue thread
     static_assert(TN * NOUT == 64, "a C tile is 64 doubles wide");
+    static_assert(NOUT * S * TN <= 448, "the S accumulators of a tile fit in TMEM");
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int kk = sa.kk;
-    const int S = sa.slices;
-    const int a_bytes = TM * kk;                // one slice of the A tile
-    const int b_bytes = TN * kk;                // one slice of one B tile
+    constexpr int kk = KK;
+    constexpr int a_bytes = TM * kk;            // one slice of the A tile
+    constexpr int b_bytes = TN * kk;            // one slice of one B tile
     unsigned char *sC = smem;                                   // 2 x 64 KB, 1024-aligned
     unsigned char *sA = sC + 2 * kCTileBytes;
     unsigned char *sB = sA + kSplitMaxSlices * a_bytes;
@@ -394,12 +399,16 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
                 if (ok && it >= 1) ok = mbar_wait_bounded(mb(5), (it - 1) & 1);
                 if (!ok) break;
                 tc_fence_after();
+#pragma unroll
                 for (int o = 0; o < NOUT; o++) {
+#pragma unroll
                     for (int l = 0; l < S; l++) {
                         const uint32_t dcol = (uint32_t)((o * S + l) * TN);
+#pragma unroll
                         for (int i = 0; i <= l; i++) {
                             const uint64_t ad = adesc0 + (uint64_t)((i * a_bytes) >> 4);
                             const uint64_t bd = bdesc0 + (uint64_t)(((o * kSplitMaxSlices + (l - i)) * b_bytes) >> 4);
+#pragma unroll
                             for (int kc = 0; kc < kk / 32; kc++)
                                 mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
                                        (i > 0 || kc > 0) ? 1u : 0u);
@@ -459,34 +468,35 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             if (!ok) break;
             tc_fence_after();
             unsigned char *cb = sC + buf * kCTileBytes;
-            // 8 logical columns at a time
+            // all of this thread's TMEM values first, folded to one double per
+            // output: the accumulators go back to the MMA thread before the
+            // shared-memory update, so the next tile's MMAs overlap it
+            double dv[NOUT][CW];
 #pragma unroll
             for (int c8 = 0; c8 < CW / 8; c8++) {
-                double dv[NOUT][8];
 #pragma unroll
                 for (int o = 0; o < NOUT; o++) {
-                    int32_t v[kSplitMaxSlices][8];
+                    int32_t v[S][8];
 #pragma unroll
-                    for (int l = 0; l < kSplitMaxSlices; l++)
-                        if (l < S)
-                            tmem_ld8(tmem + ((uint32_t)(quarter * 32) << 16) +
-                                         (uint32_t)((o * S + l) * TN + h * CW + c8 * 8), v[l]);
+                    for (int l = 0; l < S; l++)
+                        tmem_ld8(tmem + ((uint32_t)(quarter * 32) << 16) +
+                                     (uint32_t)((o * S + l) * TN + h * CW + c8 * 8), v[l]);
                     tmem_ld_wait();
 #pragma unroll
                     for (int c = 0; c < 8; c++) {
                         int32_t P[kSplitMaxSlices];
 #pragma unroll
-                        for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l][c] : 0;
-                        dv[o][c] = fold_levels(P);
+                        for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l < S ? l : 0][c] : 0;
+                        dv[o][c8 * 8 + c] = fold_levels(P);
                     }
                 }
-                if (c8 == CW / 8 - 1) {
-                    // every TMEM read of this tile is done: the MMA thread may go on
-                    tc_fence_before();
-                    mbar_arrive(mb(5));
-                }
-                // read-modify-write of the 8 * NOUT doubles in shared memory:
-                // C += value * 2^(ea + eb - 56), one rounding
+            }
+            tc_fence_before();
+            mbar_arrive(mb(5));
+            // read-modify-write of the CW * NOUT doubles in shared memory:
+            // C += value * 2^(ea + eb - 56), one rounding
+#pragma unroll
+            for (int c8 = 0; c8 < CW / 8; c8++) {
                 double sc[8];
 #pragma unroll
                 for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
@@ -496,11 +506,11 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
                     double2 *pp = reinterpret_cast<double2 *>(cb + cswz(r, d0 + 2 * pr));
                     double2 old = *pp;
                     if (NOUT == 1) {
-                        old.x = fma(dv[0][2 * pr], sc[2 * pr], old.x);
-                        old.y = fma(dv[0][2 * pr + 1], sc[2 * pr + 1], old.y);
+                        old.x = fma(dv[0][c8 * 8 + 2 * pr], sc[2 * pr], old.x);
+                        old.y = fma(dv[0][c8 * 8 + 2 * pr + 1], sc[2 * pr + 1], old.y);
                     } else {
-                        old.x = fma(dv[0][pr], sc[pr], old.x);
-                        old.y = fma(dv[NOUT - 1][pr], sc[pr], old.y);
+                        old.x = fma(dv[0][c8 * 8 + pr], sc[pr], old.x);
+                        old.y = fma(dv[NOUT - 1][c8 * 8 + pr], sc[pr], old.y);
                     }
                     *pp = old;
                 }
@@ -584,7 +594,7 @@ static bool make_c_map(CUtensorMap *map, void *W, int n, int nout, int64_t batch
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int TN, int NOUT>
+template <int TN, int NOUT, int KK, int S>
 static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
                           cudaStream_t stream)
 {
@@ -602,12 +612,29 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     if (per < 1) per = 1;
     CUtensorMap map;
     if (!make_c_map(&map, W, n, NOUT, batch)) return PFB_ERR_UNSUPPORTED;
-    auto k = split_update_kernel<TN, NOUT>;
-    const size_t smem = split_smem_bytes<TN, NOUT>(sa.kk);
+    auto k = split_update_kernel<TN, NOUT, KK, S>;
+    const size_t smem = split_smem_bytes<TN, NOUT>(KK);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PFB_ERR_CUDA;
     k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(map, n, k0, K, st, sa);
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+}
+
+// one instantiation per (operand width, slices): the MMA issue unrolls
+template <int TN, int NOUT, int KK>
+static int launch_split_s(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
+                          cudaStream_t stream)
+{
+    switch (sa.slices) {
+    case 1: return launch_split_t<TN, NOUT, KK, 1>(W, n, k0, K, batch, st, sa, stream);
+    case 2: return launch_split_t<TN, NOUT, KK, 2>(W, n, k0, K, batch, st, sa, stream);
+    case 3: return launch_split_t<TN, NOUT, KK, 3>(W, n, k0, K, batch, st, sa, stream);
+    case 4: return launch_split_t<TN, NOUT, KK, 4>(W, n, k0, K, batch, st, sa, stream);
+    case 5: return launch_split_t<TN, NOUT, KK, 5>(W, n, k0, K, batch, st, sa, stream);
+    case 6: return launch_split_t<TN, NOUT, KK, 6>(W, n, k0, K, batch, st, sa, stream);
+    case 7: return launch_split_t<TN, NOUT, KK, 7>(W, n, k0, K, batch, st, sa, stream);
+    default: return PFB_ERR_INVALID;
+    }
 }
 
 int launch_split_update(bool cplx, void *W, int n, int k0, int K, int64_t batch, MatState *st,
@@ -615,8 +642,13 @@ int launch_split_update(bool cplx, void *W, int n, int k0, int K, int64_t batch,
 {
     if (n - (k0 + K) <= 0) return PFB_OK;
     // NOUT * S levels * TN columns <= 448 of the 512 TMEM columns
-    if (!cplx) return launch_split_t<64, 1>(W, n, k0, K, batch, st, sa, stream);
-    return launch_split_t<32, 2>(W, n, k0, K, batch, st, sa, stream);
+    if (cplx) {
+        if (sa.kk != 64) return PFB_ERR_INVALID;
+        return launch_split_s<32, 2, 64>(W, n, k0, K, batch, st, sa, stream);
+    }
+    if (sa.kk == 64) return launch_split_s<64, 1, 64>(W, n, k0, K, batch, st, sa, stream);
+    if (sa.kk == 32) return launch_split_s<64, 1, 32>(W, n, k0, K, batch, st, sa, stream);
+    return PFB_ERR_INVALID;
 }
 
 }  // namespace pfb
