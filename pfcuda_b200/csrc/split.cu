@@ -40,7 +40,8 @@
 
 namespace pfb {
 
-constexpr int kSplitThreads = 320;   // warp 0: loads, warp 1: MMA, warps 2-9: epilogue
+constexpr int kSplitThreads = 576;   // warp 0: loads, warp 1: MMA, warps 2-17: epilogue
+constexpr int kEpiThreads = 512;
 constexpr long long kWaitSpins = 1LL << 24;   // bounded mbarrier polling
 
 bool split_available()
@@ -208,15 +209,15 @@ PFB_D void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memor
 PFB_D void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 PFB_D void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 PFB_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-PFB_D void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-// AND of p over the 256 epilogue threads (a barrier all of them reach), so that
+PFB_D void epi_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+// AND of p over the 512 epilogue threads (a barrier all of them reach), so that
 // a timed-out wait ends the loop of every epilogue thread together
 PFB_D bool epi_all(bool p)
 {
     uint32_t r;
     asm volatile("{\n\t.reg .pred pi, po;\n\t"
                  "setp.ne.u32 pi, %1, 0;\n\t"
-                 "bar.red.and.pred po, 1, 256, pi;\n\t"
+                 "bar.red.and.pred po, 1, 512, pi;\n\t"
                  "selp.u32 %0, 1, 0, po;\n\t}"
                  : "=r"(r) : "r"((uint32_t)p) : "memory");
     return r != 0;
@@ -260,8 +261,10 @@ PFB_D uint32_t cswz(int r, int d)
 // of one matrix's trailing block (blockIdx.y = matrix, blockIdx.x = CTA):
 //   warp 0   bulk copies of the int8 operand chunks,
 //   warp 1   one thread issues the tcgen05 MMAs,
-//   warps 2-9  epilogue: warp w reads TMEM lane quarter w%4 (the only one it
-//            may access) and the half h = (w-2)/4 of the tile's columns.
+//   warps 2-17 epilogue: warp w reads TMEM lane quarter w%4 (the only one it
+//            may access) and column group h = (w-2)/4 of the tile (16 of
+//            its 64 doubles, one C box); four warps per lane quarter hide
+//            the latencies of the TMEM reads and the shared-memory update.
 // The FP64 tile of W (C) travels by TMA in both directions: one epilogue
 // thread loads the tile after next into one of two shared buffers while the
 // current one is updated in place, then stores it back with a bulk tensor store
@@ -288,7 +291,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
 {
     constexpr int TM = kSplitTileM;
     constexpr uint32_t TMEM_COLS = 512;
-    constexpr int CW = TN / 2;                  // logical columns per epilogue thread
+    constexpr int CW = TN / 4;                  // logical columns per epilogue thread
     static_assert(TN * NOUT == 64, "a C tile is 64 doubles wide");
     static_assert(NOUT * S * TN <= 448, "the S accumulators of a tile fit in TMEM");
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -323,7 +326,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     const uint32_t bar0 = su32(bars);
     auto mb = [bar0](int i) { return bar0 + 8u * (uint32_t)i; };
     if (tid == 0) {
-        for (int i = 0; i < 8; i++) mbar_init(mb(i), i == 5 ? 256u : 1u);
+        for (int i = 0; i < 8; i++) mbar_init(mb(i), i == 5 ? (uint32_t)kEpiThreads : 1u);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *s_fail = 0;
     }
@@ -422,10 +425,10 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             if (!ok) atomicExch(s_fail, 1);
         }
     } else {
-        // ---------------- epilogue (warps 2-9), thread = tile row
+        // ---------------- epilogue (warps 2-17), thread = tile row
         const bool leader = tid == 64;
         const int quarter = warp & 3;
-        const int h = (warp - 2) >> 2;
+        const int h = (warp - 2) >> 2;              // column group: 16 doubles = one C box
         const int r = quarter * 32 + lane;          // row within the tile
         const int bz = (int)b;
         TileWalk tw{ntn, R, 0, 0};
@@ -450,17 +453,11 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
         for (int it = 0; it < ntiles && ok; it++) {
             const int buf = it & 1;
             // this tile's scale exponents, loaded before the waits: the row's
-            // own, and lane c's the one of column c of this thread's half
+            // own, and lane c's the one of column c of this thread's group
             const int arow = k1 + tw.I * TM + r;
             const int bc0 = k1 + tw.J * TN + h * CW;
             const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
             const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
-            if (leader && it >= 1 && it + 1 < ntiles) {
-                // the store of tile it-1 has read its buffer: load tile it+1 there
-                bulk_wait_read0();
-                tl.next();
-                PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
-            }
             bool w_ok = mbar_wait_bounded(mb(6 + buf), (it >> 1) & 1);
             if (w_ok) c_done = it + 1;
             if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1);
@@ -493,6 +490,12 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             }
             tc_fence_before();
             mbar_arrive(mb(5));
+            if (leader && it >= 1 && it + 1 < ntiles) {
+                // the store of tile it-1 has long read its buffer: load tile it+1 there
+                bulk_wait_read0();
+                tl.next();
+                PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
+            }
             // read-modify-write of the CW * NOUT doubles in shared memory:
             // C += value * 2^(ea + eb - 56), one rounding
 #pragma unroll
@@ -500,7 +503,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
                 double sc[8];
 #pragma unroll
                 for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
-                const int d0 = h * 32 + c8 * 8 * NOUT;
+                const int d0 = h * 16 + c8 * 8 * NOUT;
 #pragma unroll
                 for (int pr = 0; pr < 4 * NOUT; pr++) {
                     double2 *pp = reinterpret_cast<double2 *>(cb + cswz(r, d0 + 2 * pr));
