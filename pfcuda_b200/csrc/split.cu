@@ -231,18 +231,26 @@ PFB_D double exp2i(int e)
     return scalbn(1.0, e);
 }
 
+// An integer |v| < 2^51 as a double, exactly, by the usual magic-number
+// construction (integer add, one FP64 subtraction): it keeps the conversions
+// off the transcendental/conversion pipe, which otherwise limits the epilogue.
+PFB_D double i2d_exact(long long v)
+{
+    return __longlong_as_double(v + 0x4338000000000000LL) - 0x1.8p52;
+}
+
 // sum_l P_l 2^(7(6-l)) for the S <= 7 digit levels of one output (|P_l| < 2^23):
 // adjacent levels pair up exactly in int32 (P_l * 2^7 + P_(l+1) < 2^31), the
-// first FP64 step is exact (< 2^46), the last two round.  The rounding is far
-// below the splitting's own truncation (K * 2^-49 relative).
+// pairs into H = Q01 2^14 + Q23 (< 2^46) and L = Q45 2^7 + P_6 (< 2^38) in
+// int64, and the value H 2^21 + L is formed with a single rounding.
 PFB_D double fold_levels(const int32_t (&P)[kSplitMaxSlices])
 {
     const int32_t q01 = P[0] * 128 + P[1];
     const int32_t q23 = P[2] * 128 + P[3];
     const int32_t q45 = P[4] * 128 + P[5];
-    double t = fma((double)q01, 0x1p14, (double)q23);
-    t = fma(t, 0x1p14, (double)q45);
-    return fma(t, 0x1p7, (double)P[6]);
+    const long long hi = ((long long)q01 << 14) + q23;
+    const long long lo = ((long long)q45 << 7) + P[6];
+    return fma(i2d_exact(hi), 0x1p21, i2d_exact(lo));
 }
 
 // The C tile (128 rows x 64 doubles) moves as 4 boxes of 16 doubles x 128 rows
