@@ -78,6 +78,14 @@ PFB_D double neg(double x) { return -x; }
 
 // ----------------------------------------------------------------- panel
 
+// A CTA's best candidate as pushed to every CTA of the cluster: the value
+// (whose modulus is the key) and its column, in one 16- or 32-byte store.
+template <typename T>
+struct alignas(16) PivHdr {
+    T val;
+    int col;
+};
+
 template <typename T, int NB>
 struct PanelSmem {
     using Real = typename RealOf<T>::type;
@@ -85,17 +93,41 @@ struct PanelSmem {
     static constexpr int NW = NT / 32;
     T lb[NB][NB + 1];                  // replicated NB x NB block of the panel columns
     alignas(16) T stage[2][NB];        // this CTA's best trailing column, panel rows 0..NB-1
-    T hval[2][kClusterMax];            // per-CTA best candidate, pushed by every CTA of the cluster
-    Real hkey[2][kClusterMax];
-    int hcol[2][kClusterMax];
+    PivHdr<T> hdr[2][kClusterMax];     // per-CTA best candidate, pushed by every CTA of the cluster
     T wval[NW];                        // per-warp best candidate
-    Real wkey[NW];
+    unsigned long long wkey[NW];       // its key as bits
     int wcol[NW];
     T pivval[NB / 2];                  // this panel's pivots and pivot columns
     int pivcol[NB / 2];
 };
 
 template <typename T> PFB_D void put(uint32_t a, T v) { st_remote(a, v); }
+
+PFB_D void put_hdr(uint32_t a, double v, int col)
+{
+    const long long b = __double_as_longlong(v);
+    asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %3};"
+                 ::"r"(a), "r"((int)(b & 0xffffffffLL)), "r"((int)(b >> 32)), "r"(col) : "memory");
+}
+PFB_D void put_hdr(uint32_t a, c128 v, int col)
+{
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.re), "d"(v.im) : "memory");
+    asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(a + 16), "r"(col) : "memory");
+}
+
+// The first maximum of (key, column) over a warp: the largest key (compared
+// as the bits of a non-negative double, high word then low word) and, among
+// equal keys, the smallest column.  Three warp reductions.
+PFB_D void warp_argmax(unsigned long long kb, int col, unsigned long long &wkb, int &wcol)
+{
+    const unsigned hi = (unsigned)(kb >> 32), lo = (unsigned)kb;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const unsigned mc = __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? (unsigned)col : 0xffffffffu);
+    wkb = ((unsigned long long)mhi << 32) | mlo;
+    wcol = (int)mc;
+}
+PFB_D unsigned long long key_bits(double k) { return (unsigned long long)__double_as_longlong(k); }
 PFB_D void store_pair(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
 PFB_D void store_pair(c128 *p, c128 a, c128 b) { p[0] = a; p[1] = b; }
 
@@ -138,6 +170,7 @@ PFB_D T lazy_panel(const T (*lb)[NB + 1], T s, int r, int c, int t)
 {
     T s2 = zero<T>(), s3 = zero<T>(), s4 = zero<T>();
     int u = 0;
+#pragma unroll 4
     for (; u + 1 < t; u += 2) {
         s = fma_(lb[2 * u][r], lb[2 * u + 1][c], s);
         s2 = fms_(lb[2 * u + 1][r], lb[2 * u][c], s2);
@@ -262,46 +295,40 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         }
 
         // (2) this thread's best candidate (its panel column first: the
-        // smaller index), then the warp's
-        Real key = (Real)(-1);
+        // smaller index), then the warp's.  A thread without candidates has
+        // key 0 and column INT_MAX, so it loses every tie.
+        unsigned long long kb = 0;
         int col = INT_MAX;
         int qsel = -1;
         T val = zero<T>();
-        if (pcand) { key = pkey(pv); col = pc; val = pv; }
+        if (pcand) { kb = key_bits(pkey(pv)); col = pc; val = pv; }
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
             if (cq[q] < n) {
-                Real kq = pkey(Rw[q][0]);
-                if (kq > key) { key = kq; col = cq[q]; qsel = q; val = Rw[q][0]; }
+                const unsigned long long kq = key_bits(pkey(Rw[q][0]));
+                if (kq > kb || col == INT_MAX) { kb = kq; col = cq[q]; qsel = q; val = Rw[q][0]; }
             }
         }
-        Real wk = key;
-        int wc = col;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            Real k2 = shfl_xor(wk, off);
-            int c2 = shfl_xor(wc, off);
-            if (k2 > wk || (k2 == wk && c2 < wc)) { wk = k2; wc = c2; }
-        }
+        unsigned long long wk;
+        int wc;
+        warp_argmax(kb, col, wk, wc);
         if (wc != INT_MAX && col == wc) sm.wval[warp] = val;
         if (lane == 0) { sm.wkey[warp] = wk; sm.wcol[warp] = wc; }
         __syncthreads();
 
         // (3) the CTA's best candidate: its header goes to every CTA of the
         // cluster, and if it is a trailing column its owner stages the column
-        Real ck = (Real)(-1);
+        unsigned long long ck = 0;
         int cc = INT_MAX, cw = 0;
 #pragma unroll
         for (int w = 0; w < NW; w++) {
-            Real kk = sm.wkey[w];
-            int c = sm.wcol[w];
+            const unsigned long long kk = sm.wkey[w];
+            const int c = sm.wcol[w];
             if (kk > ck || (kk == ck && c < cc)) { ck = kk; cc = c; cw = w; }
         }
-        if (tid < CL) {
-            put(map_rank(smem_u32(&sm.hkey[par][rank]), tid), ck);
-            put(map_rank(smem_u32(&sm.hcol[par][rank]), tid), cc);
-            put(map_rank(smem_u32(&sm.hval[par][rank]), tid), sm.wval[cw]);
-        }
+        // (a CTA without candidates sends key 0 and column INT_MAX)
+        if (tid < CL)
+            put_hdr(map_rank(smem_u32(&sm.hdr[par][rank]), tid), cc == INT_MAX ? zero<T>() : sm.wval[cw], cc);
         if (qsel >= 0 && col == cc) {
 #pragma unroll
             for (int P = 0; P < NB / 2; P++) {
@@ -318,20 +345,16 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         }
         cluster_sync();
 
-        // (4) the pivot: a butterfly over the CL <= 16 headers, lane s of every
-        // warp reading header s (registers stay free for the window)
-        Real hk = lane < CL ? sm.hkey[par][lane] : (Real)(-1);
-        int hc = lane < CL ? sm.hcol[par][lane] : INT_MAX;
-        int hs = lane;
-#pragma unroll
-        for (int off = kClusterMax / 2; off > 0; off >>= 1) {
-            const Real k2 = shfl_xor(hk, off);
-            const int c2 = shfl_xor(hc, off);
-            const int s2 = shfl_xor(hs, off);
-            if (k2 > hk || (k2 == hk && c2 < hc)) { hk = k2; hc = c2; hs = s2; }
-        }
-        const int j = shfl(hc, 0), gs = shfl(hs, 0);
-        const T a = sm.hval[par][gs];
+        // (4) the pivot: the first maximum over the CL <= 16 headers, lane s of
+        // every warp reading header s
+        T hv = zero<T>();
+        int hc = INT_MAX;
+        if (lane < CL) { hv = sm.hdr[par][lane].val; hc = sm.hdr[par][lane].col; }
+        unsigned long long hk;
+        int j;
+        warp_argmax(lane < CL ? key_bits(pkey(hv)) : 0ull, hc, hk, j);
+        const int gs = __ffs(__ballot_sync(0xffffffffu, lane < CL && hc == j)) - 1;
+        const T a = shfl(hv, gs);
         if (is_zero(a) || j == INT_MAX) { dead = true; break; }
 
         // (5) interchange k+1 <-> j on the upper triangle.  The trailing rows'
@@ -380,12 +403,13 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                             else Rw[q][p] = neg(sm.lb[2 * t + 1][r]);
                         }
                     } else if (c < n) {
-                        const T old = Rw[q][1];
-                        T *pp = (c < j) ? &W[(int64_t)c * n + j] : &W[(int64_t)j * n + c];
+                        // the old row k+1 entry goes to this slot in (6), after the
+                        // load has returned: a store queued behind a load of the
+                        // same address would hold this thread here
+                        const T *pp = (c < j) ? &W[(int64_t)c * n + j] : &W[(int64_t)j * n + c];
                         gl[q] = ldcg(pp);
                         gneg[q] = c < j;
                         guse[q] = true;
-                        stcg(pp, c < j ? neg(old) : old);
                     }
                 }
                 if (has_panel)
@@ -407,15 +431,21 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
             __syncthreads();
             parity ^= 1;
         }
-#pragma unroll
-        for (int q = 0; q < CPT; q++)
-            if (guse[q]) Rw[q][1] = gneg[q] ? neg(gl[q]) : gl[q];
 
         // (6) lazy update of row k+1, then u = row_k / a, w = -row_{k+1}
         const T ia = recip(a);
 #pragma unroll
         for (int q = 0; q < CPT; q++) {
-            Rw[q][1] = neg(lazy_row<T, NB>(Rw[q][1], Rw[q], sm.lb, 2 * t + 1, fin0));
+            // the lazy sum first, the interchanged entry (a global load in
+            // flight) last: its latency hides behind the sum
+            T s1 = lazy_row<T, NB>(guse[q] ? zero<T>() : Rw[q][1], Rw[q], sm.lb, 2 * t + 1, fin0);
+            if (guse[q]) {
+                s1 = s1 + (gneg[q] ? neg(gl[q]) : gl[q]);
+                const int c = cq[q];
+                T *pp = (c < j) ? &W[(int64_t)c * n + j] : &W[(int64_t)j * n + c];
+                stcg(pp, gneg[q] ? neg(Rw[q][1]) : Rw[q][1]);
+            }
+            Rw[q][1] = neg(s1);
             Rw[q][0] = Rw[q][0] * ia;
         }
         if (has_panel && tid > 2 * t + 1 && pc < n) {
