@@ -603,17 +603,30 @@ def main():
     # panel: the panel rows are read and written once per panel
     panel_bytes = 2.0 * (n * n / 2.0) * esz * B
     dominant = "panel" if panel_ms >= upd_ms else "update"
+    # DRAM read+write bytes over algorithmic bytes for one launch of each kernel,
+    # from ncu captures (--set full) of 2n = 4096 float64, batch 2: panel_kernel
+    # at k0 = 128 (19.44 MB against 8.13 MB: the interchanged row is read down a
+    # column, a 32-byte sector per element), split_update_kernel and
+    # gemm_fp64_kernel at k0 = 320 (177 / 166 MB against 228 MB: part of the
+    # written tiles is still in L2 when the launch ends)
+    traffic_ratio = {"panel_kernel": 2.39, "split_update_kernel": 0.78, "gemm_fp64_kernel": 0.73}
     if dominant == "panel":
         achieved = panel_bytes / (panel_ms * 1e-3) / 1e9
         roof = {"kernel": "panel_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "note": "latency-bound (one cluster barrier and one global round trip per pivot pair); "
-                        "algorithmic bytes = panel rows read and written once"}
+                "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic_ratio["panel_kernel"] * panel_bytes / npan,
+                "note": "latency-bound: 32 dependent pivot steps per launch, each a cluster barrier and a "
+                        "global load of the interchanged row (~7k cycles per step); algorithmic bytes = "
+                        "panel rows read and written once; traffic per launch scaled from ncu"}
     else:
+        kname = "split_update_kernel" if head == "split" else "gemm_fp64_kernel"
         achieved = upd_bytes / (upd_ms * 1e-3) / 1e9
-        roof = {"kernel": "split_update_kernel" if head == "split" else "gemm_fp64_kernel", "bound": "hbm",
+        roof = {"kernel": kname, "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": None, "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch"}
+                "traffic": traffic_ratio[kname] * upd_bytes / max(npan - 1, 1),
+                "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch; "
+                        "traffic per launch scaled from ncu"}
+    roof["peak_source"] = "MEASURED_PEAKS.json hbm_gbs (measured)"
     line = {
         "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
