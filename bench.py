@@ -6,7 +6,7 @@ matrix, 2n = 4096, float64, A = (G - G^T)/2 with G ~ N(0, 1/2n) from seed 1
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
 A step is one pfb_slog_pfaffian call on a batch of independent matrices (as
-many as the GPU factors concurrently: 8 at 2n = 4096) through the C ABI; the
+many as the GPU factors concurrently: 7 at 2n = 4096) through the C ABI; the
 batch-1 latency of each path is reported beside it.  `value` is the
 split-precision path (int8 slices on the tcgen05 tensor cores, FP64 panel) when
 it is available, else the FP64 path; the other path is timed in the same run
@@ -415,12 +415,14 @@ def _hbm_peak():
         return 6650.0
 
 
-def auto_batch(n):
-    """Matrices factored concurrently per call: as many panel clusters as the
-    GPU runs at once (a cluster of ceil((n-64)/256) CTAs per matrix, at most one
-    16-CTA cluster per GPC)."""
-    cl = max(1, -(-(n - 64) // 256))
-    return max(1, min(16, 128 // max(cl, 8) if cl >= 8 else 16))
+def auto_batch(n, dtype="float64"):
+    """Matrices factored concurrently per call: as many panel clusters (one per
+    matrix) as the GPU keeps resident at once, from the occupancy calculator
+    (pfb_slog_max_concurrent); 16 where the panels are small."""
+    from pfcuda_b200 import _lib
+    dt = _lib.F64 if dtype == "float64" else _lib.C128
+    m = int(_lib.lib().pfb_slog_max_concurrent(dt, n))
+    return max(1, min(16, m)) if m > 0 else 8
 
 
 def main():
@@ -458,7 +460,7 @@ def main():
         return
 
     n = args.n
-    B = args.batch if args.batch > 0 else auto_batch(n)
+    B = args.batch if args.batch > 0 else auto_batch(n, args.dtype)
     npdt = np.float64 if args.dtype == "float64" else np.complex128
     A_host = O.config_large(n, dtype=npdt, seed=1 + rank, B=B)
     A = torch.from_numpy(A_host).to(dev)

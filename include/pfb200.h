@@ -129,6 +129,16 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
 int pfb_slog_panel_width(int dtype, int n);
 
 /*
+ * How many matrices of order n the current device factors concurrently: the
+ * number of panel thread-block clusters (one per matrix, up to 16 CTAs) that
+ * can be resident at once for the widest panel of the factorisation, as the
+ * CUDA occupancy calculator reports it (7 on a B200 for 2n = 4096).  A batch of
+ * this many matrices keeps every panel in one wave.  Returns 0 for orders the
+ * large path does not take, or without a device.  No reference counterpart.
+ */
+int pfb_slog_max_concurrent(int dtype, int n);
+
+/*
  * (log|Pf|, sign) of a ragged batch in one launch: `count` matrices of even (or
  * odd) orders n[i] <= max_n <= PFB_RAGGED_MAX_N, each float32 or float64
  * (dtype[i]), each contiguous at A[i] in `layout`.  A, n and dtype are DEVICE

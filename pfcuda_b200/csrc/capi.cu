@@ -67,6 +67,12 @@ int pfb_slog_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout
                                    workspace_bytes, stream, nullptr);
 }
 
+int pfb_slog_max_concurrent(int dtype, int n)
+{
+    if (!valid_dtype(dtype) || n <= 32) return 0;
+    return pfb::large_max_concurrent(dtype, n);
+}
+
 int pfb_slog_panel_width(int dtype, int n)
 {
     if (!valid_dtype(dtype) || n < 0) return 0;

@@ -367,6 +367,41 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
+template <typename T, int NB, int CPT>
+static int max_concurrent_t(int n)
+{
+    const int mt = n - NB;
+    int CL = mt > 0 ? (mt + kTT * CPT - 1) / (kTT * CPT) : 1;
+    if (CL < 1) CL = 1;
+    auto pk = panel_kernel<T, NB, CPT>;
+    const size_t psmem = sizeof(PanelSmem<T, NB>);
+    if (cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(pk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 0;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)CL, 1, 1);
+    cfg.blockDim = dim3(kTT, 1, 1);
+    cfg.dynamicSmemBytes = psmem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, pk, &cfg) != cudaSuccess) return 0;
+    return num;
+}
+
+int large_max_concurrent(int dtype, int n)
+{
+    int nb = 0, cpt = 0;
+    if (!large_cfg(dtype, n, &nb, &cpt)) return 0;
+    const bool cplx = dtype == PFB_C64 || dtype == PFB_C128;
+    if (!cplx) return nb == 64 ? max_concurrent_t<double, 64, 1>(n) : max_concurrent_t<double, 32, 2>(n);
+    return max_concurrent_t<c128, 32, 1>(n);
+}
+
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
                  cudaStream_t stream, const pfb_slog_timing *timing)

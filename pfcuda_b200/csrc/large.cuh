@@ -25,6 +25,7 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
                  cudaStream_t stream, const pfb_slog_timing *timing);
 
 int large_panel_width(int dtype, int n);
+int large_max_concurrent(int dtype, int n);
 
 // Where the factorisation leaves its results inside a large-path workspace:
 // the pivot columns (n/2 per matrix), the per-matrix state, and W, the

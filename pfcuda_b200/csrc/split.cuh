@@ -54,10 +54,34 @@ PFB_D void split_store16(int8_t *base, const SplitArgs &sa, int64_t b, int s, in
     *reinterpret_cast<int4 *>(p) = *reinterpret_cast<const int4 *>(d);
 }
 
+// |d| < 2^51 truncated toward zero, as an integer, without the conversion
+// pipe: the magic-number addition rounds to nearest (exactly), then one step
+// back toward zero if that went past d.
+PFB_D long long trunc_to_int(double d)
+{
+    const double big = 0x1.8p52;
+    long long x = __double_as_longlong(d + big) - 0x4338000000000000LL;
+    const double r = (d + big) - big;
+    if (d >= 0.0) { if (r > d) x -= 1; }
+    else { if (r < d) x += 1; }
+    return x;
+}
+
+// Digit s (0 = most significant) of the 49-bit truncated magnitude, signed.
+PFB_D int8_t digit_of(long long x, int s)
+{
+    const long long m = x < 0 ? -x : x;
+    const int d = (int)((m >> (42 - 7 * s)) & 127);
+    return (int8_t)(x < 0 ? -d : d);
+}
+
 // Slice one trailing column's K panel values into `slices` int8 digits with a
-// shared power-of-two scale (Ozaki's error-free splitting: every digit and
-// every remainder is exact in FP64).  Y's digits are X's with each (u, w) pair
-// mapped to (w, -u).  R is consumed (overwritten by the remainders).
+// shared power-of-two scale (Ozaki's error-free splitting): with e the exponent
+// of the column's largest magnitude, every value x becomes
+// X = trunc(x 2^(49-e)) (|X| < 2^49, exact: a power-of-two scaling and a
+// truncation), and digit s is bits 42-7s .. 48-7s of |X| with x's sign -- the
+// same digits as repeated "multiply by 128, truncate, keep the remainder".
+// Y's digits are X's with each (u, w) pair mapped to (w, -u).
 template <typename T, int NB>
 PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R)[NB], int K)
 {
@@ -66,32 +90,25 @@ PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R
     double mx = 0.0;
 #pragma unroll
     for (int r = 0; r < NB; r++) {
+        if (r >= K) R[r] = zero<T>();
         if constexpr (IsComplex<T>::value) mx = fmax(mx, fmax(fabs(R[r].re), fabs(R[r].im)));
         else mx = fmax(mx, fabs(R[r]));
     }
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);          // mx < 2^e
     sa.ex[b * sa.n + a] = e;
-    const double sc = ldexp(1.0, -e);
+    const double sc = ldexp(1.0, 49 - e);
 #pragma unroll
-    for (int r = 0; r < NB; r++) {
-        if (r >= K) R[r] = zero<T>();
-        if constexpr (IsComplex<T>::value) { R[r].re *= sc; R[r].im *= sc; }
-        else R[r] *= sc;
-    }
-    for (int s = 0; s < sa.slices; s++) {
+    for (int kc = 0; kc < NB / 16; kc++) {
         if constexpr (!IsComplex<T>::value) {
+            long long X[16];
 #pragma unroll
-            for (int kc = 0; kc < NB / 16; kc++) {
+            for (int r = 0; r < 16; r++) X[r] = trunc_to_int(R[16 * kc + r] * sc);
+            for (int s = 0; s < sa.slices; s++) {
                 alignas(16) int8_t dx[16];
                 alignas(16) int8_t dy[16];
 #pragma unroll
-                for (int r = 0; r < 16; r++) {
-                    const double v = R[16 * kc + r] * 128.0;
-                    const double d = trunc(v);
-                    R[16 * kc + r] = v - d;
-                    dx[r] = (int8_t)d;
-                }
+                for (int r = 0; r < 16; r++) dx[r] = digit_of(X[r], s);
 #pragma unroll
                 for (int r = 0; r < 16; r += 2) {   // (u, w) -> (w, -u)
                     dy[r] = dx[r + 1];
@@ -102,8 +119,13 @@ PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R
             }
         } else {
             // A = [Xr | Xi],  B1 = [Yr | -Yi],  B2 = [Yi | Yr]:  Re = A.B1, Im = A.B2
+            long long Xr[16], Xi[16];
 #pragma unroll
-            for (int kc = 0; kc < NB / 16; kc++) {
+            for (int r = 0; r < 16; r++) {
+                Xr[r] = trunc_to_int(R[16 * kc + r].re * sc);
+                Xi[r] = trunc_to_int(R[16 * kc + r].im * sc);
+            }
+            for (int s = 0; s < sa.slices; s++) {
                 alignas(16) int8_t xr[16];
                 alignas(16) int8_t xi[16];
                 alignas(16) int8_t yr[16];
@@ -111,14 +133,8 @@ PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R
                 alignas(16) int8_t t[16];
 #pragma unroll
                 for (int r = 0; r < 16; r++) {
-                    double v = R[16 * kc + r].re * 128.0;
-                    double d = trunc(v);
-                    R[16 * kc + r].re = v - d;
-                    xr[r] = (int8_t)d;
-                    v = R[16 * kc + r].im * 128.0;
-                    d = trunc(v);
-                    R[16 * kc + r].im = v - d;
-                    xi[r] = (int8_t)d;
+                    xr[r] = digit_of(Xr[r], s);
+                    xi[r] = digit_of(Xi[r], s);
                 }
 #pragma unroll
                 for (int r = 0; r < 16; r += 2) {
