@@ -163,3 +163,30 @@ def test_ill_conditioned(mode):
     la, sg = la.cpu().numpy(), sg.cpu().numpy()
     assert np.all(np.abs(la - logs) <= 1e-10 * np.abs(logs))
     assert np.array_equal(sg, signs)
+
+
+@pytest.mark.parametrize("n,cplx", [(4200, False), (6144, False), (3000, True), (4128, True)])
+def test_widest_configurations(n, cplx):
+    """The 32-row panels with two columns per thread (real 2n > 4160) and the
+    complex panels up to their limit: log|Pf| = (1/2) log|det A| (NumPy's LU on
+    the host) in both modes, split within 1e-10 of FP64, a unit sign."""
+    A = O.config_large(n, dtype=np.complex128 if cplx else np.float64, seed=11)
+    got = {}
+    for mode in MODES:
+        la, sg, piv = pf.slog_pfaffian_raw(cuda(A), mode=mode, return_pivots=True)
+        got[mode] = (la.cpu().numpy(), sg.cpu().numpy(), piv.cpu().numpy())
+    s, ld = np.linalg.slogdet(A[0])
+    for mode in MODES:
+        la = got[mode][0][0]
+        assert abs(2 * la - ld) <= 1e-10 * abs(ld), (mode, 2 * la, ld)
+    assert abs(got["split"][0][0] - got["fp64"][0][0]) <= 1e-10 * abs(got["fp64"][0][0])
+    assert np.all(np.abs(np.abs(got["split"][1]) - 1) < 1e-10)
+
+
+def test_max_concurrent_query():
+    L = _lib.lib()
+    for n in (64, 1024, 4096, 8000):
+        m = L.pfb_slog_max_concurrent(_lib.F64, n)
+        assert m >= 1
+    assert L.pfb_slog_max_concurrent(_lib.F64, 16) == 0          # small path
+    assert L.pfb_slog_max_concurrent(_lib.F64, 1 << 20) == 0     # beyond the large path
