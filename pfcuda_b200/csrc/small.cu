@@ -51,6 +51,28 @@ template <typename T> struct PhaseAcc { using type = T; };
 template <> struct PhaseAcc<c64> { using type = c128; };
 template <> struct PhaseAcc<float> { using type = double; };
 
+// The two pivot rows' entries of one column, broadcast to the group together.
+template <typename T>
+struct alignas(2 * sizeof(T)) XYPair {
+    T x, y;
+};
+
+// R[1] <-> R[q] for a q in [LO, HI) that is the same for the whole warp: a
+// binary search of uniform branches down to one register swap.
+template <int LO, int HI, typename T, int G>
+PFB_D void swap_row_at(T (&R)[G], int q)
+{
+    if constexpr (HI - LO == 1) {
+        const T t = R[1];
+        R[1] = R[LO];
+        R[LO] = t;
+    } else {
+        constexpr int MID = (LO + HI) / 2;
+        if (q < MID) swap_row_at<LO, MID>(R, q);
+        else swap_row_at<MID, HI>(R, q);
+    }
+}
+
 // One group of G lanes per matrix.  OUT_SLOG selects (log|Pf|, sign) output
 // instead of the plain product.
 //
@@ -68,15 +90,13 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
     using Ph = typename PhaseAcc<T>::type;
     constexpr int MPW = 32 / G;   // matrices per warp
 
-    __shared__ T s_x[kSmallWarps][32];
-    __shared__ T s_y[kSmallWarps][32];
+    __shared__ XYPair<T> s_xy[kSmallWarps][32];
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int gl = lane % G;            // lane within the group = initial column
     const int grp = lane / G;
-    T *X = &s_x[warp][grp * G];
-    T *Y = &s_y[warp][grp * G];
+    XYPair<T> *XY = &s_xy[warp][grp * G];
     const unsigned gmask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
 
     const int64_t nn = (int64_t)n * n;
@@ -120,10 +140,15 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
             // update below (window position q = j - k takes the old row k+1,
             // row k+1 becomes the old row j)
             const int q = j - k;
-            const T r1 = R[1];
-            T rq = r1;
+            T r1 = R[1], rq = r1;
+            if constexpr (G == 32) {
+                // one matrix per warp: q is warp-uniform, the rows swap in place
+                if (q >= 2 && q < G) swap_row_at<2, G>(R, q);
+                rq = R[1];
+            } else {
 #pragma unroll
-            for (int p = 2; p < G; p++) rq = (p == q) ? R[p] : rq;
+                for (int p = 2; p < G; p++) rq = (p == q) ? R[p] : rq;
+            }
             if (!dead && j != k + 1) {
                 lbl = (lbl == k + 1) ? j : ((lbl == j) ? k + 1 : lbl);
                 swaps ^= 1;
@@ -139,8 +164,7 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
 
             // ---- rank-2 Schur update S[r][c] -= (x_r y_c - y_r x_c) / a, row
             // k+2+p into window position p
-            X[lbl] = R[0];
-            Y[lbl] = rq;
+            XY[lbl] = XYPair<T>{R[0], rq};
             __syncwarp();
             if (!dead && lbl > k + 1 && lbl < n) {
                 const T ia = recip(a);
@@ -153,8 +177,12 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
 #pragma unroll
                     for (int p = p0; p < p0 + 4 && p < G - 2; p++) {
                         const int r = k + 2 + p;
-                        const T old = (p + 2 == q) ? r1 : R[p + 2];
-                        if (r < n) R[p] = fma_(Y[r], xh, fms_(X[r], yh, old));
+                        // (G = 32 swapped already; otherwise position q takes the old row k+1)
+                        const T old = (G < 32 && p + 2 == q) ? r1 : R[p + 2];
+                        if (r < n) {
+                            const XYPair<T> v = XY[r];
+                            R[p] = fma_(v.y, xh, fms_(v.x, yh, old));
+                        }
                     }
                     asm volatile("" ::: "memory");
                 }
