@@ -318,14 +318,14 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
 
         // (3) the CTA's best candidate: its header goes to every CTA of the
         // cluster, and if it is a trailing column its owner stages the column
-        unsigned long long ck = 0;
-        int cc = INT_MAX, cw = 0;
-#pragma unroll
-        for (int w = 0; w < NW; w++) {
-            const unsigned long long kk = sm.wkey[w];
-            const int c = sm.wcol[w];
-            if (kk > ck || (kk == ck && c < cc)) { ck = kk; cc = c; cw = w; }
-        }
+        // (the same warp reductions over the NW warp results, lane w reading warp w's)
+        const unsigned long long wkl = lane < NW ? sm.wkey[lane] : 0ull;
+        const int wcl = lane < NW ? sm.wcol[lane] : INT_MAX;
+        unsigned long long ck;
+        int cc;
+        warp_argmax(wkl, wcl, ck, cc);
+        int cw = __ffs(__ballot_sync(0xffffffffu, lane < NW && wcl == cc && wkl == ck)) - 1;
+        cw = cw < 0 ? 0 : cw;
         // (a CTA without candidates sends key 0 and column INT_MAX)
         if (tid < CL)
             put_hdr(map_rank(smem_u32(&sm.hdr[par][rank]), tid), cc == INT_MAX ? zero<T>() : sm.wval[cw], cc);
