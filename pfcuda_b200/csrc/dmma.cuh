@@ -1,0 +1,119 @@
+// dmma.cuh -- FP64 tensor-core (DMMA) pieces of the skew rank-K trailing
+// updates
+//     S[a][b] += sum_r X[r][a] * Y[r][b],   Y[2s] = X[2s+1], Y[2s+1] = -X[2s],
+// X = the K panel rows (real FP64).  One warp-wide mma.sync m8n8k4 does 256
+// fused multiply-adds from two operand registers per lane, so the operand
+// traffic from shared memory is a small fraction of the FFMA form's and the
+// FP64 pipe, not the shared-memory port, bounds the update.
+#pragma once
+#include "common.cuh"
+
+namespace pfb {
+
+// D = A (8 x 4) * B (4 x 8) + D in FP64.  Lane l = 4g + t holds
+// a = A[g][t], b = B[t][g] and d = D[g][2t .. 2t+1].
+PFB_D void dmma_884(double (&d)[2], double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
+// 16-byte asynchronous global -> shared copy; the destination is zero-filled
+// when !ok (src is then not read).
+PFB_D void cp_async16(void *dst_smem, const void *src, bool ok)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(ok ? 16 : 0)
+                 : "memory");
+}
+PFB_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> PFB_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Upper-triangle block (I, J), J >= I, of an nb x nb block grid from its
+// linear index (row-major over the upper triangle).
+PFB_D void upper_block(int idx, int nb, int &I, int &J)
+{
+    int i = 0;
+    while (idx >= nb - i) {
+        idx -= nb - i;
+        i++;
+    }
+    I = i;
+    J = i + idx;
+}
+
+// C fragments of an (8*MI) x (8*NJ) block with top-left (a0, b0) of the
+// row-major n x n matrix W: lane (g, t) of fragment (i, j) holds
+// W[a0 + 8i + g][b0 + 8j + 2t .. +1]; zero outside the matrix.  (n and b0
+// even, so the pair is 16-byte aligned and lies wholly inside or outside.)
+template <int MI, int NJ>
+PFB_D void load_c_frags(double (&c)[MI][NJ][2], const double *__restrict__ W, int n, int a0, int b0)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const int ar = a0 + 8 * i + g;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            const int bc = b0 + 8 * j + 2 * t;
+            if (ar < n && bc < n) {
+                const double2 v = *reinterpret_cast<const double2 *>(W + (int64_t)ar * n + bc);
+                c[i][j][0] = v.x;
+                c[i][j][1] = v.y;
+            } else {
+                c[i][j][0] = 0.0;
+                c[i][j][1] = 0.0;
+            }
+        }
+    }
+}
+
+// Store of the fragments back, strictly above the diagonal only (the lower
+// triangle of the working matrix is never read).
+template <int MI, int NJ>
+PFB_D void store_c_frags(const double (&c)[MI][NJ][2], double *__restrict__ W, int n, int a0, int b0)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const int ar = a0 + 8 * i + g;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            const int bc = b0 + 8 * j + 2 * t;
+            if (ar < n && bc < n) {
+                double *p = W + (int64_t)ar * n + bc;
+                if (bc > ar) *reinterpret_cast<double2 *>(p) = make_double2(c[i][j][0], c[i][j][1]);
+                else if (bc == ar) p[1] = c[i][j][1];
+            }
+        }
+    }
+}
+
+// One k-step of 4 panel rows (kb, a multiple of 4): c += X^T Y over the
+// (8*MI) x (8*NJ) block.  xs points at X[kb][a-offset], ys at the rows that
+// Y is made of, X[kb][b-offset]; ld is the row stride of both, in doubles.
+// Lane (g, t) reads X[kb+t][8i+g] and Y[kb+t][8j+g] = +-X[(kb+t)^1][8j+g]
+// (negative for odd rows, i.e. odd t).  A row stride of 8 (mod 16) doubles
+// makes each fragment read two conflict-free shared-memory wavefronts.
+template <int MI, int NJ>
+PFB_D void dmma_kstep(double (&c)[MI][NJ][2], const double *xs, const double *ys, int ld)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+    const double *xr = xs + t * ld + g;
+    const double *yr = ys + (t ^ 1) * ld + g;
+    double af[MI], bf[NJ];
+#pragma unroll
+    for (int i = 0; i < MI; i++) af[i] = xr[8 * i];
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        const double v = yr[8 * j];
+        bf[j] = (t & 1) ? -v : v;
+    }
+#pragma unroll
+    for (int i = 0; i < MI; i++)
+#pragma unroll
+        for (int j = 0; j < NJ; j++) dmma_884(c[i][j], af[i], bf[j]);
+}
+
+}  // namespace pfb

@@ -29,8 +29,9 @@
 //     reference's recurrence restricted to the panel's own Gauss vectors.
 //   * trailing update: S22 += X^T Y on the upper-triangle tiles, X = the NB panel
 //     rows (u/w interleaved), Y = the same rows with each (u, w) pair replaced by
-//     (w, -u) -- a skew rank-NB update, FP64 here (gemm_fp64_kernel) or
-//     error-free int8 slices on the tcgen05 tensor cores (split.cu).
+//     (w, -u) -- a skew rank-NB update, in FP64 on the FP64 tensor cores
+//     (gemm_dmma_kernel; complex: gemm_fp64_kernel, FFMA) or in error-free
+//     int8 slices on the tcgen05 tensor cores (split.cu).
 //   * finalize: log/sign from the per-matrix state.
 // Column-major input is handled like the small path: its row-major view is the
 // transpose -A, and Pf(-A) = (-1)^(n/2) Pf(A) exactly.
@@ -40,6 +41,7 @@
 #include "large.cuh"
 #include "split.cuh"
 #include "panel.cuh"
+#include "dmma.cuh"
 
 namespace pfb {
 
@@ -216,6 +218,67 @@ gemm_fp64_kernel(T *__restrict__ W_all, int n, int k0, int K, const MatState *__
     }
 }
 
+// The same update for real FP64 on the FP64 tensor cores (dmma.cuh): one
+// 128 x 128 upper tile per 512-thread block, each of the 16 warps a 32 x 32
+// block of m8n8k4 fragments.  The C tile is loaded straight into the accumulators
+// first, so its latency overlaps the copies of the panel rows; the panel rows
+// arrive by cp.async in groups of 16 and each group is multiplied as soon as
+// it lands.  A diagonal tile reads its Y rows from its own X rows.
+constexpr int kDmmaBM = 128;
+constexpr int kDmmaLD = kDmmaBM + 8;   // row stride in shared memory (8 mod 16 doubles)
+constexpr int kDmmaThreads = 512;
+
+template <int KMAX>
+__global__ void __launch_bounds__(kDmmaThreads, 1)
+gemm_dmma_kernel(double *__restrict__ W_all, int n, int k0, int K, const MatState *__restrict__ st_all)
+{
+    constexpr int GR = 16;                 // panel rows per copy group
+    constexpr int NG = KMAX / GR;
+    static_assert(KMAX % GR == 0 && NG <= 4, "copy groups");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Xs = reinterpret_cast<double *>(smem_raw);   // [KMAX][kDmmaLD]: rows k0.., columns a0..
+    double *Ys = Xs + KMAX * kDmmaLD;                     // [KMAX][kDmmaLD]: rows k0.., columns b0..
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    double *W = W_all + b * (int64_t)n * n;
+    const int k1 = k0 + K;
+    const int nt = (n - k1 + kDmmaBM - 1) / kDmmaBM;
+    int I, J;
+    upper_block(blockIdx.x, nt, I, J);
+    const int a0 = k1 + I * kDmmaBM, b0 = k1 + J * kDmmaBM;
+    const bool diag = I == J;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int wa = (warp >> 2) * 32, wb = (warp & 3) * 32;   // this warp's block in the tile
+
+    double acc[4][4][2];
+    load_c_frags<4, 4>(acc, W, n, a0 + wa, b0 + wb);
+
+    constexpr int CPR = kDmmaBM / 2;       // 16-byte chunks per tile row
+    const int per_group = GR * CPR * (diag ? 1 : 2);
+#pragma unroll
+    for (int gi = 0; gi < NG; gi++) {
+        for (int e = tid; e < per_group; e += kDmmaThreads) {
+            const int side = e >= GR * CPR;              // 0: X (columns a0..), 1: Y (columns b0..)
+            const int e2 = side ? e - GR * CPR : e;
+            const int r = gi * GR + e2 / CPR, c = 2 * (e2 % CPR);
+            const int col = (side ? b0 : a0) + c;
+            const bool ok = r < K && col < n;
+            cp_async16((side ? Ys : Xs) + r * kDmmaLD + c, ok ? W + (int64_t)(k0 + r) * n + col : W, ok);
+        }
+        cp_async_commit();
+    }
+    const double *Yr = diag ? Xs : Ys;
+    static_for<0, NG, 1>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        cp_async_wait<NG - 1 - gi>();
+        __syncthreads();
+#pragma unroll 1
+        for (int kb = gi * GR; kb < gi * GR + GR; kb += 4)
+            dmma_kstep<4, 4>(acc, Xs + kb * kDmmaLD + wa, Yr + kb * kDmmaLD + wb, kDmmaLD);
+    });
+    store_c_frags<4, 4>(acc, W, n, a0 + wa, b0 + wb);
+}
+
 // ----------------------------------------------------------------- finalize
 
 // A device-side timeout of the update kernel (err != 0) yields log = NaN.
@@ -297,10 +360,10 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
         return PFB_ERR_CUDA;
 
     constexpr bool cplx = IsComplex<T>::value;
-    constexpr int BM = cplx ? 64 : 128;
-    constexpr int TM = cplx ? 4 : 8;
-    auto gk = gemm_fp64_kernel<T, BM, BM, NB, TM, TM>;
-    const size_t gsmem = (size_t)2 * NB * BM * sizeof(T);
+    // real: FP64 tensor-core tiles; complex: FFMA tiles
+    constexpr int BM = cplx ? 64 : kDmmaBM;
+    void *gk = cplx ? (void *)gemm_fp64_kernel<T, 64, 64, NB, 4, 4> : (void *)gemm_dmma_kernel<NB>;
+    const size_t gsmem = cplx ? (size_t)2 * NB * BM * sizeof(T) : (size_t)2 * NB * kDmmaLD * sizeof(double);
     if (cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem) != cudaSuccess)
         return PFB_ERR_CUDA;
 
@@ -349,7 +412,10 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
             } else {
                 const int nt = (mt + BM - 1) / BM;
                 const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
-                gk<<<dim3(tiles, (unsigned)B), 256, gsmem, s>>>(W, n, k0, K, st);
+                if constexpr (cplx)
+                    gemm_fp64_kernel<T, 64, 64, NB, 4, 4><<<dim3(tiles, (unsigned)B), 256, gsmem, s>>>(W, n, k0, K, st);
+                else
+                    gemm_dmma_kernel<NB><<<dim3(tiles, (unsigned)B), kDmmaThreads, gsmem, s>>>(W, n, k0, K, st);
                 if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
             }
             rec(tm ? tm->update_events : nullptr, 2 * panel_idx + 1);

@@ -11,20 +11,21 @@
 //   * ragged_kernel: one CTA per SM takes the next matrix from a device work
 //     counter and factors it alone: copy into its private FP64 working matrix,
 //     then for each 32-row panel the panel factorisation of large.cu run by a
-//     single CTA (panel_body with a cluster of one) followed by an in-CTA FP64
-//     skew rank-32 update of the upper trailing tiles, which stay in L2.
+//     single CTA (panel_body with a cluster of one) followed by an in-CTA
+//     skew rank-32 update of the upper trailing block on the FP64 tensor cores.
 // Nothing in the call synchronises the host or allocates, so a caller can
 // capture it in a CUDA graph and replay it.
 #include "common.cuh"
 #include "large.cuh"
 #include "panel.cuh"
+#include "dmma.cuh"
 
 namespace pfb {
 
 constexpr int kRaggedNB = 32;        // panel width
 constexpr int kRaggedCPT = 2;        // trailing columns per thread: orders up to 32 + 2*256
 constexpr int kRaggedMaxCTAs = 160;  // workspace is sized for this many CTAs
-constexpr int kUpdTile = 64;         // in-CTA update tile (64 x 64, K = 32)
+constexpr int kStripLD = PFB_RAGGED_MAX_N - kRaggedNB + 8;   // staged row stride (8 mod 16 doubles)
 
 struct RaggedLayout {
     size_t order_off, counter_off, cta_off, cta_bytes, w_off, st_off, piv_off, total;
@@ -84,64 +85,62 @@ ragged_order_kernel(const int32_t *__restrict__ ns, int64_t count, int32_t *__re
     }
 }
 
-// In-CTA FP64 update of the upper trailing tiles after the panel at k0:
-// S22[a][b] += sum_r X[r][a] Y[r][b], X = panel rows, Y[2s] = X[2s+1],
-// Y[2s+1] = -X[2s].  64 x 64 tiles, 4 x 4 outputs per thread.
-PFB_D void cta_update(double *__restrict__ W, int n, int k0, int K, double (*Xs)[kUpdTile],
-                      double (*Ys)[kUpdTile])
+// In-CTA update of the upper trailing block after the panel at k0 on the FP64
+// tensor cores: S22[a][b] += sum_r X[r][a] Y[r][b], X = panel rows, Y[2s] =
+// X[2s+1], Y[2s+1] = -X[2s] (dmma.cuh).  The K panel rows (columns k1..n) are
+// staged once in shared memory; then each warp walks its own 32 x 32 output
+// blocks of the upper triangle, the next block's C loads in flight while the
+// current block's m8n8k4 products run.
+__device__ __noinline__ void cta_update(double *__restrict__ W, int n, int k0, int K, double (*P)[kStripLD])
 {
     const int k1 = k0 + K;
     const int m = n - k1;
     if (m <= 0) return;
-    const int nt = (m + kUpdTile - 1) / kUpdTile;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    for (int I = 0; I < nt; I++) {
-        for (int J = I; J < nt; J++) {
-            const int a0 = k1 + I * kUpdTile, b0 = k1 + J * kUpdTile;
-            for (int e = tid; e < K * kUpdTile; e += kTT) {
-                const int r = e / kUpdTile, x = e % kUpdTile;
-                Xs[r][x] = (a0 + x < n) ? W[(int64_t)(k0 + r) * n + a0 + x] : 0.0;
-                const double y = (b0 + x < n) ? W[(int64_t)(k0 + (r ^ 1)) * n + b0 + x] : 0.0;
-                Ys[r][x] = (r & 1) ? -y : y;
-            }
-            __syncthreads();
-            double acc[4][4] = {};
-            for (int r = 0; r < K; r++) {
-                double xa[4], yb[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) xa[i] = Xs[r][ty + 16 * i];
-#pragma unroll
-                for (int j = 0; j < 4; j++) yb[j] = Ys[r][tx + 16 * j];
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int j = 0; j < 4; j++) acc[i][j] = fma(xa[i], yb[j], acc[i][j]);
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const int ar = a0 + ty + 16 * i;
-                if (ar >= n) continue;
-                double cv[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int bc = b0 + tx + 16 * j;
-                    cv[j] = (bc < n && bc > ar) ? W[(int64_t)ar * n + bc] : 0.0;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int bc = b0 + tx + 16 * j;
-                    if (bc < n && bc > ar) W[(int64_t)ar * n + bc] = cv[j] + acc[i][j];
-                }
-            }
-            __syncthreads();
+    const int mp = (m + 31) & ~31;       // staged width; zero beyond n
+    const int half = mp / 2;             // 16-byte chunks per staged row
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int e = tid; e < kRaggedNB * half; e += kTT) {
+        const int r = e / half, c = 2 * (e - r * half);
+        const bool ok = r < K && k1 + c < n;
+        cp_async16(&P[r][c], ok ? W + (int64_t)(k0 + r) * n + k1 + c : W, ok);
+    }
+    cp_async_commit();
+    const int nb = mp / 32;
+    const int items = nb * (nb + 1) / 2;
+    int it = warp, I = 0, J = 0;
+    double acc[4][4][2], nxt[4][4][2];
+    if (it < items) {
+        upper_block(it, nb, I, J);
+        load_c_frags<4, 4>(acc, W, n, k1 + 32 * I, k1 + 32 * J);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    while (it < items) {
+        const int nx = it + kTT / 32;
+        int In = 0, Jn = 0;
+        if (nx < items) {
+            upper_block(nx, nb, In, Jn);
+            load_c_frags<4, 4>(nxt, W, n, k1 + 32 * In, k1 + 32 * Jn);
         }
+#pragma unroll 1
+        for (int kb = 0; kb < kRaggedNB; kb += 4) dmma_kstep<4, 4>(acc, &P[kb][32 * I], &P[kb][32 * J], kStripLD);
+        store_c_frags<4, 4>(acc, W, n, k1 + 32 * I, k1 + 32 * J);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                acc[i][j][0] = nxt[i][j][0];
+                acc[i][j][1] = nxt[i][j][1];
+            }
+        I = In;
+        J = Jn;
+        it = nx;
     }
 }
 
 struct RaggedSmem {
     PanelSmem<double, kRaggedNB> panel;
-    double xs[kRaggedNB][kUpdTile];
-    double ys[kRaggedNB][kUpdTile];
+    alignas(16) double strip[kRaggedNB][kStripLD];   // the panel rows for the trailing update
     int item;
 };
 
@@ -204,7 +203,7 @@ ragged_kernel(const void *const *__restrict__ As, const int32_t *__restrict__ ns
             panel_body<double, kRaggedNB, kRaggedCPT>(sm.panel, W, n, k0, st, piv, nosplit, 0);
             if (st->dead) break;
             const int K = (n - k0 < kRaggedNB) ? n - k0 : kRaggedNB;
-            cta_update(W, n, k0, K, sm.xs, sm.ys);
+            cta_update(W, n, k0, K, sm.strip);
             __syncthreads();
         }
         if (tid == 0) {
