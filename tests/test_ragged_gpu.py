@@ -50,6 +50,38 @@ def test_edge_orders():
     check(mats, la, sg)
 
 
+def test_edge_orders_narrow_panels():
+    """Batches whose largest order is at most 528 run two CTAs per SM with
+    16-row panels; 528 fills every trailing column of the first panel."""
+    rng = np.random.default_rng(15)
+    mats = []
+    for n in (2, 4, 14, 16, 18, 30, 32, 34, 48, 50, 510, 512, 526, 528):
+        G = rng.normal(size=(n, n)) / np.sqrt(n)
+        mats.append((G - G.T) / 2)
+    la, sg = pf.slog_pfaffian_ragged([torch.from_numpy(A).cuda() for A in mats])
+    check(mats, la, sg)
+    # one order above 528 moves the whole batch to the 32-row configuration
+    G = rng.normal(size=(530, 530)) / np.sqrt(530)
+    mats.append((G - G.T) / 2)
+    la, sg = pf.slog_pfaffian_ragged([torch.from_numpy(A).cuda() for A in mats])
+    check(mats, la, sg)
+
+
+def test_unaligned_inputs():
+    """Matrices that start off a 16-byte boundary take the element-wise copy."""
+    rng = np.random.default_rng(16)
+    mats, views = [], []
+    for n, dt, off in ((64, np.float64, 1), (66, np.float32, 1), (130, np.float32, 2), (96, np.float64, 0)):
+        G = rng.normal(size=(n, n)) / np.sqrt(n)
+        A = ((G - G.T) / 2).astype(dt)
+        buf = torch.zeros(n * n + 4, dtype=torch.from_numpy(A).dtype, device="cuda")
+        buf[off:off + n * n] = torch.from_numpy(A.reshape(-1)).cuda()
+        mats.append(A)
+        views.append(buf[off:off + n * n].view(n, n))
+    la, sg = pf.slog_pfaffian_ragged(views)
+    check(mats, la, sg)
+
+
 def test_odd_zero_singular():
     rng = np.random.default_rng(6)
     G = rng.normal(size=(40, 40)) / 6
