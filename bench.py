@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--n", type=int, default=N_DEFAULT)
     p.add_argument("--dtype", default="float64", choices=["float64", "complex128"])
     p.add_argument("--mode", default="auto", choices=["auto", "split", "fp64"])
-    p.add_argument("--batch", type=int, default=0, help="matrices per call (0: as many as run concurrently)")
+    p.add_argument("--batch", type=int, default=0, help="matrices per call (0: four waves of concurrently resident panel clusters)")
     p.add_argument("--workloads", default="all",
                    choices=["all", "headline", "small", "ragged", "grad", "illcond"],
                    help="'all': the headline line plus the other workloads under 'workloads'; "
@@ -416,13 +416,19 @@ def _hbm_peak():
 
 
 def auto_batch(n, dtype="float64"):
-    """Matrices factored concurrently per call: as many panel clusters (one per
-    matrix) as the GPU keeps resident at once, from the occupancy calculator
-    (pfb_slog_max_concurrent); 16 where the panels are small."""
+    """The saturating batch: four waves of panel clusters (one cluster per
+    matrix; pfb_slog_max_concurrent of them resident at once), at most 4 GB of
+    input.  Each panel launch pays a fixed fill cost that one wave does not
+    amortise: at 2n = 4096 float64 (7 clusters per wave) split mode runs 453,
+    555, 597 and 608 matrices/s at 7, 14, 21 and 28 matrices per call."""
     from pfcuda_b200 import _lib
     dt = _lib.F64 if dtype == "float64" else _lib.C128
     m = int(_lib.lib().pfb_slog_max_concurrent(dt, n))
-    return max(1, min(16, m)) if m > 0 else 8
+    if m <= 0:
+        return 8
+    elem = 8 if dtype == "float64" else 16
+    cap = max(1, int(4e9 // (n * n * elem)))
+    return max(1, min(4 * m, cap))
 
 
 def main():
