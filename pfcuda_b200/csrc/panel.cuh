@@ -476,15 +476,28 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         cluster_sync();
         return;
     }
-    if (leader) {
-        for (int s2 = 0; s2 < t; s2++) {
-            const T a = sm.pivval[s2];
-            piv[k0 / 2 + s2] = sm.pivcol[s2];
+    // this panel's pivots (t <= NB/2 <= 32): lane s of warp 0 of rank 0 takes
+    // pivot s, then one warp tree sums the logs and multiplies the phases
+    if (rank == 0 && warp == 0) {
+        double lg = 0.0, ar = 1.0, ai = 0.0;
+        if (lane < t) {
+            const T a = sm.pivval[lane];
+            piv[k0 / 2 + lane] = sm.pivcol[lane];
             const double m = (double)mag(a);
-            la += log(m);
-            double ar, ai;
+            lg = log(m);
             if constexpr (IsComplex<T>::value) { ar = a.re / m; ai = a.im / m; }
-            else { ar = a < 0 ? -1.0 : 1.0; ai = 0.0; }
+            else { ar = a < 0 ? -1.0 : 1.0; }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            lg += shfl_xor(lg, off);
+            const double br = shfl_xor(ar, off), bi = shfl_xor(ai, off);
+            const double nr = ar * br - ai * bi, ni = ar * bi + ai * br;
+            ar = nr;
+            ai = ni;
+        }
+        if (leader) {
+            la += lg;
             const double nr = pre * ar - pim * ai, ni = pre * ai + pim * ar;
             pre = nr;
             pim = ni;
