@@ -94,8 +94,10 @@ PFB_D void store_c_frags(const double (&c)[MI][NJ][2], double *__restrict__ W, i
 // (8*MI) x (8*NJ) block.  xs points at X[kb][a-offset], ys at the rows that
 // Y is made of, X[kb][b-offset]; ld is the row stride of both, in doubles.
 // Lane (g, t) reads X[kb+t][8i+g] and Y[kb+t][8j+g] = +-X[(kb+t)^1][8j+g]
-// (negative for odd rows, i.e. odd t).  A row stride of 8 (mod 16) doubles
-// makes each fragment read two conflict-free shared-memory wavefronts.
+// (negative for odd rows, i.e. odd t).  An 8-byte shared load is served per
+// half-warp (g < 4, then g >= 4: four rows of four doubles each); a row stride
+// of 4 (mod 16) doubles puts the four rows on distinct banks, so each fragment
+// read is two conflict-free wavefronts.
 template <int MI, int NJ>
 PFB_D void dmma_kstep(double (&c)[MI][NJ][2], const double *xs, const double *ys, int ld)
 {

@@ -225,7 +225,7 @@ gemm_fp64_kernel(T *__restrict__ W_all, int n, int k0, int K, const MatState *__
 // arrive by cp.async in groups of 16 and each group is multiplied as soon as
 // it lands.  A diagonal tile reads its Y rows from its own X rows.
 constexpr int kDmmaBM = 128;
-constexpr int kDmmaLD = kDmmaBM + 8;   // row stride in shared memory (8 mod 16 doubles)
+constexpr int kDmmaLD = kDmmaBM + 4;   // row stride in shared memory (4 mod 16 doubles)
 constexpr int kDmmaThreads = 512;
 
 template <int KMAX>

@@ -30,8 +30,8 @@ namespace pfb {
 
 constexpr int kRaggedCPT = 2;        // trailing columns per thread (2 x 256 threads)
 constexpr int kRaggedMaxCTAs = 320;  // workspace is sized for this many CTAs
-// staged row stride of the panel rows (8 mod 16 doubles)
-template <int NB> __host__ __device__ constexpr int strip_ld() { return PFB_RAGGED_MAX_N - NB + 8; }
+// staged row stride of the panel rows (4 mod 16 doubles)
+template <int NB> __host__ __device__ constexpr int strip_ld() { return PFB_RAGGED_MAX_N - NB + 4; }
 // the two configurations: panel width, CTAs per SM, a warp's output block in the update
 template <int NB> struct RaggedCfg;
 template <> struct RaggedCfg<16> { static constexpr int kMinBlocks = 2, kUpdBlock = 16, kMaxN = 16 + 512; };
