@@ -34,6 +34,17 @@ PFB_D void cluster_sync()
                  "barrier.cluster.wait.acquire;" ::: "memory");
 }
 PFB_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// The panel's barrier: the cluster barrier, or for a panel factored by one
+// CTA alone (SOLO) a CTA barrier -- bar.sync orders the CTA's shared-memory
+// accesses, those made through its own shared::cluster window included,
+// without the cluster-scope release and acquire.
+template <bool SOLO>
+PFB_D void group_sync()
+{
+    if constexpr (SOLO) __syncthreads();
+    else cluster_sync();
+}
+
 PFB_D uint32_t map_rank(uint32_t addr, uint32_t rank)
 {
     uint32_t r;
@@ -224,8 +235,9 @@ PFB_D c128 ld_remote(uint32_t addr, c128 *)
 // best candidate (|value|, column, value) into every CTA's shared memory before
 // it, and the owner of a CTA's best trailing column stages that column; after
 // the barrier each CTA knows the pivot, and the panel-column threads read the
-// interchanged column straight from the winning CTA's stage.
-template <typename T, int NB, int CPT>
+// interchanged column straight from the winning CTA's stage.  SOLO: launched
+// as clusters of one CTA (the ragged kernel), the barrier is bar.sync.
+template <typename T, int NB, int CPT, bool SOLO = false>
 PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, MatState *__restrict__ st,
                       int32_t *__restrict__ piv, const SplitArgs &split, int64_t b)
 {
@@ -274,7 +286,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
     const int nsteps = (n - k0) / 2 < NB / 2 ? (n - k0) / 2 : NB / 2;
     // every CTA of the cluster has started (and loaded) before any shared
     // memory of another CTA is written
-    cluster_sync();
+    group_sync<SOLO>();
 
     int t = 0;
 #pragma unroll 1
@@ -343,7 +355,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                 store_pair(&sm.stage[par][r], v0, v1);
             }
         }
-        cluster_sync();
+        group_sync<SOLO>();
 
         // (4) the pivot: the first maximum over the CL <= 16 headers, lane s of
         // every warp reading header s
@@ -473,7 +485,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
 
     if (dead) {
         if (leader) st->dead = 1;
-        cluster_sync();
+        group_sync<SOLO>();
         return;
     }
     // this panel's pivots (t <= NB/2 <= 32): lane s of warp 0 of rank 0 takes
@@ -531,7 +543,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         st->ph_im = pim / m;
         st->parity = parity;
     }
-    cluster_sync();
+    group_sync<SOLO>();
 }
 
 }  // namespace pfb

@@ -253,7 +253,7 @@ ragged_kernel(const void *const *__restrict__ As, const int32_t *__restrict__ ns
         }
         __syncthreads();
         for (int k0 = 0; k0 < n - 1; k0 += NB) {
-            panel_body<double, NB, kRaggedCPT>(sm.panel, W, n, k0, st, piv, nosplit, 0);
+            panel_body<double, NB, kRaggedCPT, true>(sm.panel, W, n, k0, st, piv, nosplit, 0);
             if (st->dead) break;
             const int K = (n - k0 < NB) ? n - k0 : NB;
             cta_update<NB, RaggedCfg<NB>::kUpdBlock>(W, n, k0, K, sm.strip);
