@@ -590,7 +590,7 @@ def main():
             with torch.cuda.stream(cstream):
                 if i >= 2:
                     cstream.wait_event(done[bb])          # buffer bb is free once step i-2 is factored
-                d_in[bb].copy_(h_in, non_blocking=True)
+                pf.upload_upper(h_in, out=d_in[bb])   # the triangle the engine reads
                 copied[bb].record(cstream)
             stream.wait_event(copied[bb])
             l2, s2 = pf.slog_pfaffian_raw(d_in[bb], mode=head, workspace=wsh)
@@ -607,6 +607,12 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    # the triangle upload leaves the rest of the device buffer stale; the
+    # results must equal those of the whole matrix on the device, bit for bit
+    l_ref, s_ref = pf.slog_pfaffian_raw(A, mode=head, workspace=wsh)
+    torch.cuda.synchronize()
+    last = (args.steps - 1) & 1
+    e2e_same = bool(torch.equal(h_log[last], l_ref.cpu()) and torch.equal(h_sign[last], s_ref.cpu()))
 
     if rank != 0:
         if pg is not None:
@@ -628,9 +634,9 @@ def main():
     # from ncu captures (--set full) of 2n = 4096 float64, batch 2: panel_kernel
     # at k0 = 128 (19.44 MB against 8.13 MB: the interchanged row is read down a
     # column, a 32-byte sector per element), split_update_kernel and
-    # gemm_fp64_kernel at k0 = 320 (177 / 166 MB against 228 MB: part of the
+    # gemm_dmma_kernel at k0 = 320 (177 / 175 MB against 228 MB: part of the
     # written tiles is still in L2 when the launch ends)
-    traffic_ratio = {"panel_kernel": 2.39, "split_update_kernel": 0.78, "gemm_fp64_kernel": 0.73}
+    traffic_ratio = {"panel_kernel": 2.39, "split_update_kernel": 0.78, "gemm_dmma_kernel": 0.77}
     if dominant == "panel":
         achieved = panel_bytes / (panel_ms * 1e-3) / 1e9
         roof = {"kernel": "panel_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
@@ -640,7 +646,7 @@ def main():
                         "global load of the interchanged row (~7k cycles per step); algorithmic bytes = "
                         "panel rows read and written once; traffic per launch scaled from ncu"}
     else:
-        kname = "split_update_kernel" if head == "split" else "gemm_fp64_kernel"
+        kname = "split_update_kernel" if head == "split" else "gemm_dmma_kernel"
         achieved = upd_bytes / (upd_ms * 1e-3) / 1e9
         roof = {"kernel": kname, "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
@@ -666,9 +672,12 @@ def main():
         "kernel_ms": {"panel": panel_ms, "update": upd_ms, "panels": npan},
         "roofline": roof,
         "e2e": {"value": world * B / (e2e_ms * 1e-3), "unit": "matrices/s",
-                "h2d_bytes_per_step": B * n * n * esz, "d2h_bytes_per_step": B * (8 + esz),
-                "how": "slog_pfaffian_raw per step; pinned-host input copied every step on a copy stream, "
-                       "two device buffers so the copy of step i+1 overlaps the factorisation of step i"},
+                "h2d_bytes_per_step": pf.upload_upper_bytes(tdt, B, n), "d2h_bytes_per_step": B * (8 + esz),
+                "how": "per step: upload_upper of the pinned-host batch (the upper triangle of each "
+                       "matrix, the part the engine reads, in 256-row rectangles) on a copy stream, then "
+                       "slog_pfaffian_raw and the results back to pinned host memory; two device buffers "
+                       "so the upload of step i+1 overlaps the factorisation of step i",
+                "results_equal_device_path": e2e_same},
         "gpu_launches": args.steps * (2 + npan + (npan - 1)),
         "clocks": clocks,
     }

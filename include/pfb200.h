@@ -212,6 +212,25 @@ int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int l
 
 size_t pfb_slog_grad_workspace_bytes(int dtype, int64_t batch, int n, int mode);
 
+/*
+ * Host -> device upload of a batch for pfb_slog_pfaffian that moves only what
+ * the large path reads: in the row-major view of each matrix (either layout),
+ * the entries on and above the diagonal, as one rectangle per block of 256
+ * rows (rows [r0, r0+256) x columns [r0, n)) -- about (n^2 + 256 n) / 2
+ * elements per matrix instead of n^2.  Entries below the diagonal of A_dev are
+ * left as they were: the large path never reads them.  Orders n <= 32 (the
+ * small path, which reads whole matrices) are copied whole.  A_host: `batch`
+ * contiguous n x n matrices in host memory, page-locked for the copies to be
+ * asynchronous on `stream`; A_dev: a contiguous device array of the same
+ * shape and dtype.  No counterpart in the reference, whose handlers receive
+ * device buffers from XLA (bindings/jax_bindings.cu:19-80); its CPU path reads
+ * the same triangle (src/pfaffian_cpu.cpp:33-42).
+ */
+int pfb_upload_upper(int dtype, const void *A_host, void *A_dev, int64_t batch, int n, void *stream);
+
+/* Bytes pfb_upload_upper moves for such a batch (0 for invalid arguments). */
+size_t pfb_upload_upper_bytes(int dtype, int64_t batch, int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,9 +6,10 @@ complex64 / complex128, computed by hand-written sm_100a kernels behind the C AB
 of include/pfb200.h (libpfb200.so, built in-tree).
 """
 from .api import (pfaffian, slog_pfaffian, pfaffian_raw, slog_pfaffian_raw,
-                  slog_workspace_bytes, slog_pfaffian_ragged, RaggedPlan)
+                  slog_workspace_bytes, slog_pfaffian_ragged, RaggedPlan, upload_upper,
+                  upload_upper_bytes)
 from .grad import slog_pfaffian_grad, grad_workspace_bytes
 
 __all__ = ["pfaffian", "slog_pfaffian", "pfaffian_raw", "slog_pfaffian_raw",
            "slog_workspace_bytes", "slog_pfaffian_ragged", "RaggedPlan",
-           "slog_pfaffian_grad", "grad_workspace_bytes"]
+           "slog_pfaffian_grad", "grad_workspace_bytes", "upload_upper", "upload_upper_bytes"]

@@ -37,6 +37,8 @@ SIGNATURES = {
     "pfb_slog_pfaffian_noalloc": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp]),
     "pfb_slog_pfaffian_grad": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "pfb_slog_grad_workspace_bytes": (_sz, [_int, _i64, _int, _int]),
+    "pfb_upload_upper": (_int, [_int, _vp, _vp, _i64, _int, _vp]),
+    "pfb_upload_upper_bytes": (_sz, [_int, _i64, _int]),
 }
 
 class SlogTiming(ctypes.Structure):

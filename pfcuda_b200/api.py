@@ -147,6 +147,41 @@ def slog_pfaffian_raw(A: torch.Tensor, mode: str = "split", layout: int = _lib.R
     return la, sg
 
 
+def upload_upper(A_host: torch.Tensor, out: torch.Tensor | None = None,
+                 device: torch.device | None = None) -> torch.Tensor:
+    """Copy a contiguous (..., n, n) host batch to the device moving only what
+    ``slog_pfaffian`` reads: the upper triangle (diagonal included) of each
+    matrix's row-major view, in 256-row rectangles (pfb_upload_upper), about
+    half the bytes of a full copy.  Entries below the diagonal of the result
+    are left as they were in ``out`` (uninitialised for a new tensor) and are
+    never read by the large path; orders n <= 32 are copied whole.  The copies
+    are enqueued on the current stream and are asynchronous when ``A_host`` is
+    page-locked (``tensor.pin_memory()``)."""
+    if A_host.is_cuda:
+        raise ValueError("upload_upper copies from host memory")
+    if A_host.ndim < 2 or A_host.shape[-1] != A_host.shape[-2]:
+        raise ValueError(f"expected (..., n, n) matrices, got shape {tuple(A_host.shape)}")
+    if A_host.dtype not in _DT:
+        raise TypeError(f"unsupported dtype {A_host.dtype}")
+    if not A_host.is_contiguous():
+        raise ValueError("the host batch must be contiguous")
+    if out is None:
+        out = torch.empty(A_host.shape, dtype=A_host.dtype,
+                          device=device if device is not None else torch.device("cuda"))
+    elif out.shape != A_host.shape or out.dtype != A_host.dtype or not out.is_cuda or not out.is_contiguous():
+        raise ValueError("out must be a contiguous CUDA tensor of the host batch's shape and dtype")
+    n = A_host.shape[-1]
+    B = int(np.prod(A_host.shape[:-2])) if A_host.ndim > 2 else 1
+    st = _lib.lib().pfb_upload_upper(_DT[A_host.dtype], A_host.data_ptr(), out.data_ptr(), B, n, _stream(out))
+    _lib.check(st, "pfb_upload_upper")
+    return out
+
+
+def upload_upper_bytes(dtype: torch.dtype, batch: int, n: int) -> int:
+    """Bytes ``upload_upper`` moves for a batch of `batch` n x n matrices."""
+    return int(_lib.lib().pfb_upload_upper_bytes(_DT[dtype], batch, n))
+
+
 # ------------------------------------------------------------- ragged batches
 
 class RaggedPlan:

@@ -20,6 +20,10 @@ int cuda_status(cudaError_t e)
 
 bool valid_dtype(int d) { return d == PFB_F32 || d == PFB_F64 || d == PFB_C64 || d == PFB_C128; }
 bool valid_layout(int l) { return l == PFB_ROW_MAJOR || l == PFB_COL_MAJOR; }
+
+size_t dtype_bytes(int d) { return d == PFB_F32 ? 4 : (d == PFB_C128 ? 16 : 8); }
+
+constexpr int kUploadRows = 256;   // rows per rectangle of pfb_upload_upper
 }  // namespace
 
 extern "C" {
@@ -149,6 +153,42 @@ int pfb_slog_pfaffian_ragged(const void *const *A, const int32_t *n, const int32
                                       (cudaStream_t)stream);
     if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
     return rc;
+}
+
+size_t pfb_upload_upper_bytes(int dtype, int64_t batch, int n)
+{
+    if (!valid_dtype(dtype) || batch < 0 || n < 0) return 0;
+    const size_t es = dtype_bytes(dtype);
+    if (n <= 32) return (size_t)batch * (size_t)n * (size_t)n * es;
+    size_t per = 0;
+    for (int r0 = 0; r0 < n; r0 += kUploadRows) {
+        const int rows = n - r0 < kUploadRows ? n - r0 : kUploadRows;
+        per += (size_t)rows * (size_t)(n - r0) * es;
+    }
+    return per * (size_t)batch;
+}
+
+int pfb_upload_upper(int dtype, const void *A_host, void *A_dev, int64_t batch, int n, void *stream)
+{
+    if (!valid_dtype(dtype) || batch < 0 || n < 0) return PFB_ERR_INVALID;
+    if (batch == 0 || n == 0) return PFB_OK;
+    if (!A_host || !A_dev) return PFB_ERR_INVALID;
+    const cudaStream_t s = (cudaStream_t)stream;
+    const size_t es = dtype_bytes(dtype);
+    const size_t pitch = (size_t)n * es, mat = (size_t)n * pitch;
+    if (n <= 32)
+        return cuda_status(cudaMemcpyAsync(A_dev, A_host, (size_t)batch * mat, cudaMemcpyHostToDevice, s));
+    const char *src = static_cast<const char *>(A_host);
+    char *dst = static_cast<char *>(A_dev);
+    for (int64_t b = 0; b < batch; b++)
+        for (int r0 = 0; r0 < n; r0 += kUploadRows) {
+            const int rows = n - r0 < kUploadRows ? n - r0 : kUploadRows;
+            const size_t off = (size_t)b * mat + (size_t)r0 * pitch + (size_t)r0 * es;
+            const cudaError_t e = cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch, (size_t)(n - r0) * es,
+                                                    (size_t)rows, cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    return PFB_OK;
 }
 
 int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspace_bytes,

@@ -81,3 +81,21 @@ def test_grad_argument_checks_without_gpu():
         assert w1 > L.pfb_slog_workspace_bytes(dtype, 1, 512, 0) and w1 % 256 == 0
         assert L.pfb_slog_grad_workspace_bytes(dtype, 1, 35, 0) == 0
         assert L.pfb_slog_grad_workspace_bytes(dtype, 1, 1 << 20, 0) == 0
+
+
+def test_upload_upper_sizes_and_argument_checks_without_gpu():
+    L = _lib.lib()
+    # orders <= 32 go whole; above, one rectangle per 256 rows from the diagonal on
+    assert L.pfb_upload_upper_bytes(_lib.F64, 3, 32) == 3 * 32 * 32 * 8
+    assert L.pfb_upload_upper_bytes(_lib.F32, 2, 300) == 2 * (256 * 300 + 44 * 44) * 4
+    n = 4096
+    want = sum(256 * (n - r0) for r0 in range(0, n, 256)) * 16
+    assert L.pfb_upload_upper_bytes(_lib.C128, 1, n) == want
+    assert want < 0.54 * n * n * 16
+    assert L.pfb_upload_upper_bytes(99, 1, 64) == 0
+    assert L.pfb_upload_upper_bytes(_lib.F64, -1, 64) == 0
+    buf = ctypes.create_string_buffer(64)
+    assert L.pfb_upload_upper(99, buf, buf, 1, 4, None) == 1           # bad dtype
+    assert L.pfb_upload_upper(_lib.F64, None, buf, 1, 4, None) == 1    # no source
+    assert L.pfb_upload_upper(_lib.F64, buf, None, 1, 4, None) == 1    # no destination
+    assert L.pfb_upload_upper(_lib.F64, None, None, 0, 4, None) == 0   # empty batch
