@@ -416,11 +416,12 @@ def _hbm_peak():
 
 
 def auto_batch(n, dtype="float64"):
-    """The saturating batch: four waves of panel clusters (one cluster per
-    matrix; pfb_slog_max_concurrent of them resident at once), at most 4 GB of
-    input.  Each panel launch pays a fixed fill cost that one wave does not
-    amortise: at 2n = 4096 float64 (7 clusters per wave) split mode runs 453,
-    555, 597 and 608 matrices/s at 7, 14, 21 and 28 matrices per call."""
+    """The saturating batch: four waves of the widest panel clusters (one
+    cluster per matrix; pfb_slog_max_concurrent of them resident at once), at
+    most 4 GB of input.  Later panels use smaller clusters, so more of them fit
+    at once and a one-wave batch leaves most SMs idle there: at 2n = 4096
+    float64 (7 clusters of 16 per wave) split mode runs 453, 555, 597 and 608
+    matrices/s at 7, 14, 21 and 28 matrices per call."""
     from pfcuda_b200 import _lib
     dt = _lib.F64 if dtype == "float64" else _lib.C128
     m = int(_lib.lib().pfb_slog_max_concurrent(dt, n))
