@@ -118,4 +118,92 @@ PFB_D void dmma_kstep(double (&c)[MI][NJ][2], const double *xs, const double *ys
         for (int j = 0; j < NJ; j++) dmma_884(c[i][j], af[i], bf[j]);
 }
 
+// ---- complex128: four real products per complex product,
+//      re += ar br - ai bi,  im += ar bi + ai br.
+
+// C fragments of an (8*MI) x (8*NJ) complex block: lane (g, t) of fragment
+// (i, j) holds the real and imaginary parts of W[a0 + 8i + g][b0 + 8j + 2t .. +1]
+// (two 16-byte elements); zero outside the matrix.
+template <int MI, int NJ>
+PFB_D void load_c_frags(double (&cr)[MI][NJ][2], double (&ci)[MI][NJ][2], const c128 *__restrict__ W, int n,
+                        int a0, int b0)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const int ar = a0 + 8 * i + g;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            const int bc = b0 + 8 * j + 2 * t;
+            if (ar < n && bc < n) {
+                const double2 *p = reinterpret_cast<const double2 *>(W + (int64_t)ar * n + bc);
+                const double2 v0 = p[0], v1 = p[1];
+                cr[i][j][0] = v0.x;
+                ci[i][j][0] = v0.y;
+                cr[i][j][1] = v1.x;
+                ci[i][j][1] = v1.y;
+            } else {
+                cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+            }
+        }
+    }
+}
+
+template <int MI, int NJ>
+PFB_D void store_c_frags(const double (&cr)[MI][NJ][2], const double (&ci)[MI][NJ][2], c128 *__restrict__ W,
+                         int n, int a0, int b0)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const int ar = a0 + 8 * i + g;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            const int bc = b0 + 8 * j + 2 * t;
+            if (ar < n && bc < n) {
+                double2 *p = reinterpret_cast<double2 *>(W + (int64_t)ar * n + bc);
+                if (bc > ar) p[0] = make_double2(cr[i][j][0], ci[i][j][0]);
+                if (bc + 1 > ar) p[1] = make_double2(cr[i][j][1], ci[i][j][1]);
+            }
+        }
+    }
+}
+
+// One complex k-step of 4 rows (kb a multiple of 4): c += X^T Y over the
+// block, X and Y as for dmma_kstep (with PAIRSWAP, Y[r] = +-X[r^1]; without,
+// ys points at Y's own rows).  A 16-byte shared load is served per quarter
+// warp (two columns of four rows); a row stride of 2 (mod 8) complex elements
+// puts the eight on distinct bank groups.
+template <int MI, int NJ, bool PAIRSWAP>
+PFB_D void zdmma_kstep(double (&cr)[MI][NJ][2], double (&ci)[MI][NJ][2], const c128 *xs, const c128 *ys, int ld)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+    const c128 *xr = xs + t * ld + g;
+    const c128 *yr = ys + (PAIRSWAP ? (t ^ 1) : t) * ld + g;
+    double ar[MI], ai[MI], nai[MI], br[NJ], bi[NJ];
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const c128 v = xr[8 * i];
+        ar[i] = v.re;
+        ai[i] = v.im;
+        nai[i] = -v.im;
+    }
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        const c128 v = yr[8 * j];
+        const bool neg = PAIRSWAP && (t & 1);
+        br[j] = neg ? -v.re : v.re;
+        bi[j] = neg ? -v.im : v.im;
+    }
+#pragma unroll
+    for (int i = 0; i < MI; i++)
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            dmma_884(cr[i][j], ar[i], br[j]);
+            dmma_884(cr[i][j], nai[i], bi[j]);
+            dmma_884(ci[i][j], ar[i], bi[j]);
+            dmma_884(ci[i][j], ai[i], br[j]);
+        }
+}
+
 }  // namespace pfb

@@ -30,8 +30,8 @@
 //   * trailing update: S22 += X^T Y on the upper-triangle tiles, X = the NB panel
 //     rows (u/w interleaved), Y = the same rows with each (u, w) pair replaced by
 //     (w, -u) -- a skew rank-NB update, in FP64 on the FP64 tensor cores
-//     (gemm_dmma_kernel; complex: gemm_fp64_kernel, FFMA) or in error-free
-//     int8 slices on the tcgen05 tensor cores (split.cu).
+//     (gemm_dmma_kernel; complex: gemm_zdmma_kernel) or in error-free int8
+//     slices on the tcgen05 tensor cores (split.cu).
 //   * finalize: log/sign from the per-matrix state.
 // Column-major input is handled like the small path: its row-major view is the
 // transpose -A, and Pf(-A) = (-1)^(n/2) Pf(A) exactly.
@@ -143,82 +143,9 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
 
 // S22[a][b] += sum_t X[t][a] * Y[t][b] over the upper-triangle tiles of the
 // trailing block [k1, n), X = panel rows k0..k0+K-1, Y[2s] = X[2s+1],
-// Y[2s+1] = -X[2s].  A BM x BN tile per 256-thread block, K <= KMAX in one
-// shared-memory stage, TM x TN outputs per thread.
-template <typename T, int BM, int BN, int KMAX, int TM, int TN>
-__global__ void __launch_bounds__(256)
-gemm_fp64_kernel(T *__restrict__ W_all, int n, int k0, int K, const MatState *__restrict__ st_all)
-{
-    static_assert((BM / TM) * (BN / TN) == 256, "thread tile");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *Xs = reinterpret_cast<T *>(smem_raw);            // [KMAX][BM]
-    T *Ys = Xs + KMAX * BM;                              // [KMAX][BN]
-    const int64_t b = blockIdx.y;
-    if (st_all[b].dead) return;
-    T *W = W_all + b * (int64_t)n * n;
-    const int k1 = k0 + K;
-    const int m = n - k1;
-    const int nt = (m + BM - 1) / BM;   // BM == BN
-    // upper-triangle tile (I, J), J >= I, from the linear block index
-    int L = blockIdx.x, I = 0;
-    while (L >= nt - I) { L -= nt - I; I++; }
-    const int J = I + L;
-    const int a0 = k1 + I * BM, b0 = k1 + J * BN;
-    const int tid = threadIdx.x;
-
-    for (int e = tid; e < K * BM; e += 256) {
-        const int r = e / BM, x = e - r * BM;
-        Xs[r * BM + x] = (a0 + x < n) ? W[(int64_t)(k0 + r) * n + a0 + x] : zero<T>();
-    }
-    for (int e = tid; e < K * BN; e += 256) {
-        const int r = e / BN, y = e - r * BN;
-        T v = zero<T>();
-        if (b0 + y < n) {
-            const T s = W[(int64_t)(k0 + (r ^ 1)) * n + b0 + y];
-            v = (r & 1) ? neg(s) : s;
-        }
-        Ys[r * BN + y] = v;
-    }
-    __syncthreads();
-
-    const int tx = tid % (BN / TN), ty = tid / (BN / TN);
-    T acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; i++)
-#pragma unroll
-        for (int jj = 0; jj < TN; jj++) acc[i][jj] = zero<T>();
-
-    for (int r = 0; r < K; r++) {
-        T xa[TM], yb[TN];
-#pragma unroll
-        for (int i = 0; i < TM; i++) xa[i] = Xs[r * BM + ty + i * (BM / TM)];
-#pragma unroll
-        for (int jj = 0; jj < TN; jj++) yb[jj] = Ys[r * BN + tx + jj * (BN / TN)];
-#pragma unroll
-        for (int i = 0; i < TM; i++)
-#pragma unroll
-            for (int jj = 0; jj < TN; jj++) acc[i][jj] = fma_(xa[i], yb[jj], acc[i][jj]);
-    }
-    // per output row: all loads first, then the stores (one memory round trip per row)
-#pragma unroll
-    for (int i = 0; i < TM; i++) {
-        const int ar = a0 + ty + i * (BM / TM);
-        if (ar >= n) continue;
-        T cv[TN];
-#pragma unroll
-        for (int jj = 0; jj < TN; jj++) {
-            const int bc = b0 + tx + jj * (BN / TN);
-            cv[jj] = (bc < n && bc > ar) ? W[(int64_t)ar * n + bc] : zero<T>();
-        }
-#pragma unroll
-        for (int jj = 0; jj < TN; jj++) {
-            const int bc = b0 + tx + jj * (BN / TN);
-            if (bc < n && bc > ar) W[(int64_t)ar * n + bc] = cv[jj] + acc[i][jj];
-        }
-    }
-}
-
-// The same update for real FP64 on the FP64 tensor cores (dmma.cuh): one
+// Y[2s+1] = -X[2s] (the FP64 mode's trailing update).
+//
+// Real FP64 on the FP64 tensor cores (dmma.cuh): one
 // 128 x 128 upper tile per 512-thread block, each of the 16 warps a 32 x 32
 // block of m8n8k4 fragments.  The C tile is loaded straight into the accumulators
 // first, so its latency overlaps the copies of the panel rows; the panel rows
@@ -277,6 +204,62 @@ gemm_dmma_kernel(double *__restrict__ W_all, int n, int k0, int K, const MatStat
             dmma_kstep<4, 4>(acc, Xs + kb * kDmmaLD + wa, Yr + kb * kDmmaLD + wb, kDmmaLD);
     });
     store_c_frags<4, 4>(acc, W, n, a0 + wa, b0 + wb);
+}
+
+// The complex128 form: one 64 x 64 upper tile per 256-thread block, each warp
+// a 32 x 16 block, four real m8n8k4 products per complex product (dmma.cuh);
+// otherwise as gemm_dmma_kernel.
+constexpr int kZdmmaBM = 64;
+constexpr int kZdmmaLD = kZdmmaBM + 2;   // row stride in shared memory (2 mod 8 complex elements)
+
+template <int KMAX>
+__global__ void __launch_bounds__(256, 2)
+gemm_zdmma_kernel(c128 *__restrict__ W_all, int n, int k0, int K, const MatState *__restrict__ st_all)
+{
+    constexpr int GR = 16;                 // panel rows per copy group
+    constexpr int NG = KMAX / GR;
+    static_assert(KMAX % GR == 0 && NG <= 4, "copy groups");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    c128 *Xs = reinterpret_cast<c128 *>(smem_raw);   // [KMAX][kZdmmaLD]: rows k0.., columns a0..
+    c128 *Ys = Xs + KMAX * kZdmmaLD;                  // [KMAX][kZdmmaLD]: rows k0.., columns b0..
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    c128 *W = W_all + b * (int64_t)n * n;
+    const int k1 = k0 + K;
+    const int nt = (n - k1 + kZdmmaBM - 1) / kZdmmaBM;
+    int I, J;
+    upper_block(blockIdx.x, nt, I, J);
+    const int a0 = k1 + I * kZdmmaBM, b0 = k1 + J * kZdmmaBM;
+    const bool diag = I == J;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int wa = (warp >> 2) * 32, wb = (warp & 3) * 16;   // this warp's block in the tile
+
+    double cr[4][2][2], ci[4][2][2];
+    load_c_frags<4, 2>(cr, ci, W, n, a0 + wa, b0 + wb);
+
+    const int per_group = GR * kZdmmaBM * (diag ? 1 : 2);   // 16-byte elements
+#pragma unroll
+    for (int gi = 0; gi < NG; gi++) {
+        for (int e = tid; e < per_group; e += 256) {
+            const int side = e >= GR * kZdmmaBM;
+            const int e2 = side ? e - GR * kZdmmaBM : e;
+            const int r = gi * GR + e2 / kZdmmaBM, c = e2 % kZdmmaBM;
+            const int col = (side ? b0 : a0) + c;
+            const bool ok = r < K && col < n;
+            cp_async16((side ? Ys : Xs) + r * kZdmmaLD + c, ok ? W + (int64_t)(k0 + r) * n + col : W, ok);
+        }
+        cp_async_commit();
+    }
+    const c128 *Yr = diag ? Xs : Ys;
+    static_for<0, NG, 1>([&](auto gc) {
+        constexpr int gi = decltype(gc)::value;
+        cp_async_wait<NG - 1 - gi>();
+        __syncthreads();
+#pragma unroll 1
+        for (int kb = gi * GR; kb < gi * GR + GR; kb += 4)
+            zdmma_kstep<4, 2, true>(cr, ci, Xs + kb * kZdmmaLD + wa, Yr + kb * kZdmmaLD + wb, kZdmmaLD);
+    });
+    store_c_frags<4, 2>(cr, ci, W, n, a0 + wa, b0 + wb);
 }
 
 // ----------------------------------------------------------------- finalize
@@ -360,10 +343,17 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
         return PFB_ERR_CUDA;
 
     constexpr bool cplx = IsComplex<T>::value;
-    // real: FP64 tensor-core tiles; complex: FFMA tiles
-    constexpr int BM = cplx ? 64 : kDmmaBM;
-    void *gk = cplx ? (void *)gemm_fp64_kernel<T, 64, 64, NB, 4, 4> : (void *)gemm_dmma_kernel<NB>;
-    const size_t gsmem = cplx ? (size_t)2 * NB * BM * sizeof(T) : (size_t)2 * NB * kDmmaLD * sizeof(double);
+    // FP64 tensor-core tiles: 128 x 128 real, 64 x 64 complex
+    constexpr int BM = cplx ? kZdmmaBM : kDmmaBM;
+    void *gk;
+    size_t gsmem;
+    if constexpr (cplx) {
+        gk = (void *)gemm_zdmma_kernel<NB>;
+        gsmem = (size_t)2 * NB * kZdmmaLD * sizeof(c128);
+    } else {
+        gk = (void *)gemm_dmma_kernel<NB>;
+        gsmem = (size_t)2 * NB * kDmmaLD * sizeof(double);
+    }
     if (cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem) != cudaSuccess)
         return PFB_ERR_CUDA;
 
@@ -413,7 +403,7 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
                 const int nt = (mt + BM - 1) / BM;
                 const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
                 if constexpr (cplx)
-                    gemm_fp64_kernel<T, 64, 64, NB, 4, 4><<<dim3(tiles, (unsigned)B), 256, gsmem, s>>>(W, n, k0, K, st);
+                    gemm_zdmma_kernel<NB><<<dim3(tiles, (unsigned)B), 256, gsmem, s>>>(W, n, k0, K, st);
                 else
                     gemm_dmma_kernel<NB><<<dim3(tiles, (unsigned)B), kDmmaThreads, gsmem, s>>>(W, n, k0, K, st);
                 if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
