@@ -206,4 +206,92 @@ PFB_D void zdmma_kstep(double (&cr)[MI][NJ][2], double (&ci)[MI][NJ][2], const c
         }
 }
 
+// ---- general products c += A B (the adjoint's kernels): A and B in shared
+// memory, each either k-major (AK / BK: A[k][a], B[k][b]) or k-contiguous
+// (A[a][k], B[b][k]).  Conflict-free row strides: real, 4 (mod 16) doubles in
+// both layouts; complex, 2 (mod 8) elements k-major and 4 (mod 8)
+// k-contiguous (16-byte loads are served per quarter warp).
+
+template <int MI, int NJ, bool AK, bool BK>
+PFB_D void dmma_kstep_g(double (&c)[MI][NJ][2], const double *A, int lda, const double *B, int ldb, int kb)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+    double af[MI], bf[NJ];
+#pragma unroll
+    for (int i = 0; i < MI; i++) af[i] = AK ? A[(kb + t) * lda + 8 * i + g] : A[(8 * i + g) * lda + kb + t];
+#pragma unroll
+    for (int j = 0; j < NJ; j++) bf[j] = BK ? B[(kb + t) * ldb + 8 * j + g] : B[(8 * j + g) * ldb + kb + t];
+#pragma unroll
+    for (int i = 0; i < MI; i++)
+#pragma unroll
+        for (int j = 0; j < NJ; j++) dmma_884(c[i][j], af[i], bf[j]);
+}
+
+template <int MI, int NJ, bool AK, bool BK>
+PFB_D void zdmma_kstep_g(double (&cr)[MI][NJ][2], double (&ci)[MI][NJ][2], const c128 *A, int lda,
+                         const c128 *B, int ldb, int kb)
+{
+    const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+    double ar[MI], ai[MI], nai[MI], br[NJ], bi[NJ];
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        const c128 v = AK ? A[(kb + t) * lda + 8 * i + g] : A[(8 * i + g) * lda + kb + t];
+        ar[i] = v.re;
+        ai[i] = v.im;
+        nai[i] = -v.im;
+    }
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        const c128 v = BK ? B[(kb + t) * ldb + 8 * j + g] : B[(8 * j + g) * ldb + kb + t];
+        br[j] = v.re;
+        bi[j] = v.im;
+    }
+#pragma unroll
+    for (int i = 0; i < MI; i++)
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            dmma_884(cr[i][j], ar[i], br[j]);
+            dmma_884(cr[i][j], nai[i], bi[j]);
+            dmma_884(ci[i][j], ar[i], bi[j]);
+            dmma_884(ci[i][j], ai[i], br[j]);
+        }
+}
+
+// Accumulators of an (8*MI) x (8*NJ) block for T = double or c128, with the
+// k-step and element access the adjoint's kernels use; lane (g, t) of
+// fragment (i, j) holds elements (8i + g, 8j + 2t + e), e = 0, 1.
+template <typename T, int MI, int NJ> struct FragAcc;
+template <int MI, int NJ> struct FragAcc<double, MI, NJ> {
+    double c[MI][NJ][2];
+    PFB_D void zero()
+    {
+#pragma unroll
+        for (int i = 0; i < MI; i++)
+#pragma unroll
+            for (int j = 0; j < NJ; j++) c[i][j][0] = c[i][j][1] = 0.0;
+    }
+    template <bool AK, bool BK>
+    PFB_D void step(const double *A, int lda, const double *B, int ldb, int kb)
+    {
+        dmma_kstep_g<MI, NJ, AK, BK>(c, A, lda, B, ldb, kb);
+    }
+    PFB_D double get(int i, int j, int e) const { return c[i][j][e]; }
+};
+template <int MI, int NJ> struct FragAcc<c128, MI, NJ> {
+    double cr[MI][NJ][2], ci[MI][NJ][2];
+    PFB_D void zero()
+    {
+#pragma unroll
+        for (int i = 0; i < MI; i++)
+#pragma unroll
+            for (int j = 0; j < NJ; j++) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    }
+    template <bool AK, bool BK>
+    PFB_D void step(const c128 *A, int lda, const c128 *B, int ldb, int kb)
+    {
+        zdmma_kstep_g<MI, NJ, AK, BK>(cr, ci, A, lda, B, ldb, kb);
+    }
+    PFB_D c128 get(int i, int j, int e) const { return mk(cr[i][j][e], ci[i][j][e]); }
+};
+
 }  // namespace pfb

@@ -28,6 +28,7 @@
 //   6. grad_scatter_kernel: Q Y^T on the upper tiles, scaled and scattered to G.
 #include "common.cuh"
 #include "large.cuh"
+#include "dmma.cuh"
 
 namespace pfb {
 
@@ -151,8 +152,16 @@ grad_diag_inv_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const M
         if (j < sz) Y[(int64_t)(r0 + i) * n + r0 + j] = Ys[i * kGB + j];
 }
 
+// Shared-memory row strides of the adjoint's DMMA tiles (dmma.cuh): a
+// k-contiguous operand 32 (+4) or 64 (+4) wide, a k-major one 64 (+4 real,
+// +2 complex) wide.
+template <typename T> __host__ __device__ constexpr int ld_kc32() { return 36; }
+template <typename T> __host__ __device__ constexpr int ld_kc64() { return 68; }
+template <typename T> __host__ __device__ constexpr int ld_km64() { return IsComplex<T>::value ? 66 : 68; }
+
 // 5. one block row I of Y (rows r0 .. r0+63), column tile blockIdx.x after it:
-// Y[I][c] = -Y_II * sum_{k >= r1} U[I][k] Y[k][c]
+// Y[I][c] = -Y_II * sum_{k >= r1} U[I][k] Y[k][c], both products on the FP64
+// tensor cores (8 warps, each a 32 x 16 block of m8n8k4 fragments).
 template <typename T>
 __global__ void __launch_bounds__(256)
 grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all,
@@ -160,76 +169,67 @@ grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const 
 {
     const int64_t b = blockIdx.y;
     if (st_all[b].dead) return;
+    constexpr int LA = ld_kc32<T>(), LB = ld_km64<T>(), LY = ld_kc64<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *Ut = reinterpret_cast<T *>(smem_raw);        // [kGB][32]
-    T *Yt = Ut + kGB * 32;                           // [32][kGB]
-    T *Ts = Yt + 32 * kGB;                           // [kGB][kGB]
-    T *Yii = Ts + kGB * kGB;                         // [kGB][kGB]
+    T *Ut = reinterpret_cast<T *>(smem_raw);        // [kGB][LA]  U[I][k]   (k-contiguous)
+    T *Yt = Ut + kGB * LA;                           // [32][LB]   Y[k][c]   (k-major)
+    T *Ts = reinterpret_cast<T *>(smem_raw);        // [kGB][LB]  the sum   (k-major), after the loop
+    T *Yii = Ts + kGB * LB;                          // [kGB][LY]  Y_II      (k-contiguous)
     const T *U = U_all + b * (int64_t)n * n;
     T *Y = Y_all + b * (int64_t)n * n;
     const int r1 = r0 + kGB;
     const int c0 = r1 + blockIdx.x * kGB;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
+    const int tid = threadIdx.x, warp = tid >> 5, g = (tid & 31) >> 2, t = tid & 3;
+    const int wa = (warp >> 2) * 32, wb = (warp & 3) * 16;
+    FragAcc<T, 4, 2> acc;
+    acc.zero();
     const int kend = (c0 + kGB < n) ? c0 + kGB : n;    // Y[k][c] = 0 for k > c
     for (int k0 = r1; k0 < kend; k0 += 32) {
         for (int e = tid; e < kGB * 32; e += 256) {
             const int i = e / 32, k = e % 32;
-            Ut[e] = (r0 + i < n && k0 + k < n) ? U[(int64_t)(r0 + i) * n + k0 + k] : zero<T>();
+            Ut[i * LA + k] = (r0 + i < n && k0 + k < n) ? U[(int64_t)(r0 + i) * n + k0 + k] : zero<T>();
             const int kk = e / kGB, c = e % kGB;
-            Yt[e] = (k0 + kk < n && c0 + c < n) ? Y[(int64_t)(k0 + kk) * n + c0 + c] : zero<T>();
+            Yt[kk * LB + c] = (k0 + kk < n && c0 + c < n) ? Y[(int64_t)(k0 + kk) * n + c0 + c] : zero<T>();
         }
         __syncthreads();
-        for (int k = 0; k < 32; k++) {
-            T ua[4], yb[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) ua[i] = Ut[(ty + 16 * i) * 32 + k];
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) yb[jj] = Yt[k * kGB + tx + 16 * jj];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma_(ua[i], yb[jj], acc[i][jj]);
-        }
+#pragma unroll 1
+        for (int kb = 0; kb < 32; kb += 4) acc.template step<false, true>(Ut + wa * LA, LA, Yt + wb, LB, kb);
         __syncthreads();
     }
+    // the sum to shared memory (row = its k in the second product)
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int jj = 0; jj < 4; jj++) Ts[(ty + 16 * i) * kGB + tx + 16 * jj] = acc[i][jj];
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int e2 = 0; e2 < 2; e2++) Ts[(wa + 8 * i + g) * LB + wb + 8 * j + 2 * t + e2] = acc.get(i, j, e2);
     for (int e = tid; e < kGB * kGB; e += 256) {
         const int i = e / kGB, k = e % kGB;
-        Yii[e] = (r0 + i < n && r0 + k < n) ? Y[(int64_t)(r0 + i) * n + r0 + k] : zero<T>();
+        Yii[i * LY + k] = (r0 + i < n && r0 + k < n) ? Y[(int64_t)(r0 + i) * n + r0 + k] : zero<T>();
     }
     __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
-    for (int k = 0; k < kGB; k++) {
-        T ya[4], tb[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) ya[i] = Yii[(ty + 16 * i) * kGB + k];
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) tb[jj] = Ts[k * kGB + tx + 16 * jj];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) acc[i][jj] = fms_(ya[i], tb[jj], acc[i][jj]);
-    }
+    acc.zero();
+#pragma unroll 1
+    for (int kb = 0; kb < kGB; kb += 4) acc.template step<false, true>(Yii + wa * LY, LY, Ts + wb, LB, kb);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int r = r0 + ty + 16 * i;
+        const int r = r0 + wa + 8 * i + g;
 #pragma unroll
-        for (int jj = 0; jj < 4; jj++) {
-            const int c = c0 + tx + 16 * jj;
-            if (r < n && c < n) Y[(int64_t)r * n + c] = acc[i][jj];
-        }
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int e2 = 0; e2 < 2; e2++) {
+                const int c = c0 + wb + 8 * j + 2 * t + e2;
+                if (r < n && c < n) Y[(int64_t)r * n + c] = -acc.get(i, j, e2);
+            }
     }
+}
+
+template <typename T>
+constexpr size_t block_row_smem()
+{
+    constexpr size_t p1 = (size_t)(kGB * ld_kc32<T>() + 32 * ld_km64<T>()) * sizeof(T);
+    constexpr size_t p2 = (size_t)(kGB * ld_km64<T>() + kGB * ld_kc64<T>()) * sizeof(T);
+    return p1 > p2 ? p1 : p2;
 }
 
 template <typename T, typename O>
@@ -240,7 +240,7 @@ template <> PFB_D c128 to_out<c128, c128>(c128 v) { return v; }
 template <> PFB_D c64 to_out<c128, c64>(c128 v) { return mk((float)v.re, (float)v.im); }
 
 // 6. M = Q Y^T on the upper 64 x 64 tiles, G[perm[r]][perm[c]] = -(ct/2) M[r][c]
-// and its skew mirror.  Matrices with Pf = 0 get NaN.
+// and its skew mirror, on the FP64 tensor cores.  Matrices with Pf = 0 get NaN.
 template <typename T, typename O>
 __global__ void __launch_bounds__(256)
 grad_scatter_kernel(const T *__restrict__ W_all, const T *__restrict__ Y_all, const int32_t *__restrict__ perm_all,
@@ -253,7 +253,7 @@ grad_scatter_kernel(const T *__restrict__ W_all, const T *__restrict__ Y_all, co
     while (L >= nt - I) { L -= nt - I; I++; }
     const int J = I + L;
     const int i0 = I * kGB, j0 = J * kGB;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x;
     const int32_t *perm = perm_all + b * (int64_t)n;
     if (st_all[b].dead) {
         for (int e = tid; e < kGB * kGB; e += 256) {
@@ -268,66 +268,69 @@ grad_scatter_kernel(const T *__restrict__ W_all, const T *__restrict__ Y_all, co
         }
         return;
     }
+    constexpr int LD = ld_kc32<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int LD = kGB + 1;                     // padded: the fills below walk k across lanes
-    T *Qs = reinterpret_cast<T *>(smem_raw);       // [32][LD]  Q[i][k] for the tile's rows
-    T *Ys = Qs + 32 * LD;                           // [32][LD]  Y[j][k] for the tile's columns
+    T *Qs = reinterpret_cast<T *>(smem_raw);       // [kGB][LD]  Q[i][k] for the tile's rows (k-contiguous)
+    T *Ys = Qs + kGB * LD;                          // [kGB][LD]  Y[j][k] for the tile's columns
+    T *ias = Ys + kGB * LD;                         // [16]       1 / a_t for the chunk's 16 pivot pairs
     const T *W = W_all + b * (int64_t)n * n;
     const T *Y = Y_all + b * (int64_t)n * n;
-    T acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) acc[i][jj] = zero<T>();
+    const int warp = tid >> 5, g = (tid & 31) >> 2, t = tid & 3;
+    const int wa = (warp >> 2) * 32, wb = (warp & 3) * 16;
+    FragAcc<T, 4, 2> acc;
+    acc.zero();
     for (int k0 = j0; k0 < n; k0 += 32) {            // Y[j][k] = 0 for k < j
+        if (tid < 16) {
+            const int p = (k0 >> 1) + tid;           // k0 is even
+            ias[tid] = (2 * p + 1 < n) ? recip(W[(int64_t)(2 * p) * n + 2 * p + 1]) : zero<T>();
+        }
+        __syncthreads();
         for (int e = tid; e < 32 * kGB; e += 256) {
-            const int x = e >> 5, k = e & 31;        // consecutive lanes read consecutive k of a row
+            const int x = e >> 5, k = e & 31;        // consecutive lanes: consecutive k of a row
             const int kg = k0 + k;
             T q = zero<T>(), y = zero<T>();
             if (kg < n) {
                 if (i0 + x < n) {
-                    const int t = kg >> 1;
-                    const T ia = recip(W[(int64_t)(2 * t) * n + 2 * t + 1]);
-                    q = (kg & 1) ? (-Y[(int64_t)(i0 + x) * n + 2 * t]) * ia : Y[(int64_t)(i0 + x) * n + 2 * t + 1] * ia;
+                    const T ia = ias[k >> 1];
+                    q = (kg & 1) ? (-Y[(int64_t)(i0 + x) * n + (kg - 1)]) * ia : Y[(int64_t)(i0 + x) * n + kg + 1] * ia;
                 }
                 if (j0 + x < n) y = Y[(int64_t)(j0 + x) * n + kg];
             }
-            Qs[k * LD + x] = q;
-            Ys[k * LD + x] = y;
+            Qs[x * LD + k] = q;
+            Ys[x * LD + k] = y;
         }
         __syncthreads();
-        for (int k = 0; k < 32; k++) {
-            T qa[4], yb[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) qa[i] = Qs[k * LD + ty + 16 * i];
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) yb[jj] = Ys[k * LD + tx + 16 * jj];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int jj = 0; jj < 4; jj++) acc[i][jj] = fma_(qa[i], yb[jj], acc[i][jj]);
-        }
+#pragma unroll 1
+        for (int kb = 0; kb < 32; kb += 4) acc.template step<false, false>(Qs + wa * LD, LD, Ys + wb * LD, LD, kb);
         __syncthreads();
     }
     const double s = -0.5 * (ct ? ct[b] : 1.0);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int r = i0 + ty + 16 * i;
+        const int r = i0 + wa + 8 * i + g;
 #pragma unroll
-        for (int jj = 0; jj < 4; jj++) {
-            const int c = j0 + tx + 16 * jj;
-            if (r < n && c < n && r <= c) {
-                const int pr = perm[r], pc = perm[c];
-                if (r == c) {
-                    G[(int64_t)pr * n + pr] = to_out<T, O>(zero<T>());
-                } else {
-                    const T g = scal(acc[i][jj], s);
-                    G[(int64_t)pr * n + pc] = to_out<T, O>(g);
-                    G[(int64_t)pc * n + pr] = to_out<T, O>(-g);
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int e2 = 0; e2 < 2; e2++) {
+                const int c = j0 + wb + 8 * j + 2 * t + e2;
+                if (r < n && c < n && r <= c) {
+                    const int pr = perm[r], pc = perm[c];
+                    if (r == c) {
+                        G[(int64_t)pr * n + pr] = to_out<T, O>(zero<T>());
+                    } else {
+                        const T gv = scal(acc.get(i, j, e2), s);
+                        G[(int64_t)pr * n + pc] = to_out<T, O>(gv);
+                        G[(int64_t)pc * n + pr] = to_out<T, O>(-gv);
+                    }
                 }
             }
-        }
     }
+}
+
+template <typename T>
+constexpr size_t scatter_smem()
+{
+    return (size_t)(2 * kGB * ld_kc32<T>() + 16) * sizeof(T);
 }
 
 template <typename T>
@@ -358,7 +361,7 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
     }
     {
         auto k = grad_block_row_kernel<T>;
-        const size_t sm = (2 * kGB * 32 + 2 * kGB * kGB) * sizeof(T);
+        const size_t sm = block_row_smem<T>();
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
             return PFB_ERR_CUDA;
         for (int I = nblk - 2; I >= 0; I--) {
@@ -369,7 +372,7 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
     }
     {
         const unsigned tiles = (unsigned)(nblk * (nblk + 1) / 2);
-        const size_t sm = 2 * 32 * (kGB + 1) * sizeof(T);
+        const size_t sm = (dtype == PFB_C64 || dtype == PFB_C128) ? scatter_smem<c128>() : scatter_smem<double>();
         if (dtype == PFB_F32) {
             auto k = grad_scatter_kernel<double, float>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
