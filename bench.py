@@ -679,7 +679,7 @@ def main():
                        "slog_pfaffian_raw and the results back to pinned host memory; two device buffers "
                        "so the upload of step i+1 overlaps the factorisation of step i",
                 "results_equal_device_path": e2e_same},
-        "gpu_launches": args.steps * (2 + npan + (npan - 1)),
+        "gpu_launches": args.steps * (2 + npan + (npan - 1) * (2 if head == "split" else 1)),
         "clocks": clocks,
     }
     if world == 1:

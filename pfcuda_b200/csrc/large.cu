@@ -130,13 +130,44 @@ __global__ void copy_in_kernel(const S *__restrict__ A, T *__restrict__ W, int64
 template <typename T, int NB, int CPT>
 __global__ void __launch_bounds__(kTT, 1)
 panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all,
-             int32_t *__restrict__ piv_all, SplitArgs split)
+             int32_t *__restrict__ piv_all)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PanelSmem<T, NB> &sm = *reinterpret_cast<PanelSmem<T, NB> *>(smem_raw);
     const int64_t b = blockIdx.y;
-    panel_body<T, NB, CPT>(sm, W_all + b * (int64_t)n * n, n, k0, st_all + b, piv_all + b * (int64_t)(n / 2),
-                           split, b);
+    panel_body<T, NB, CPT>(sm, W_all + b * (int64_t)n * n, n, k0, st_all + b, piv_all + b * (int64_t)(n / 2));
+}
+
+// The int8 operand images of the split update for the panel at k0 (a full
+// panel: its NB rows of W at the trailing columns hold the Gauss vectors).
+// NB/16 adjacent threads share a trailing column, one 16-row chunk each: the
+// column's exponent is the maximum over their chunks (lane shuffles), then
+// each slices its chunk (split_chunk).  A launch of its own over every SM,
+// rather than a tail of the panel kernel on the panel's CTAs only.
+template <typename T, int NB>
+__global__ void __launch_bounds__(256)
+split_slice_kernel(const T *__restrict__ W_all, int n, int k0, const MatState *__restrict__ st_all, SplitArgs sa)
+{
+    constexpr int CH = NB / 16;        // threads per column
+    constexpr int CPB = 256 / CH;      // columns per block
+    static_assert(CH == 2 || CH == 4, "16-row chunks of a 32- or 64-row panel");
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    const int k1 = k0 + NB;
+    const int ch = threadIdx.x % CH;
+    const int c = k1 + blockIdx.x * CPB + threadIdx.x / CH;
+    const bool ok = c < n;
+    const T *W = W_all + b * (int64_t)n * n;
+    T R[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) R[r] = ok ? W[(int64_t)(k0 + 16 * ch + r) * n + c] : zero<T>();
+    double mx = max_component(R);
+#pragma unroll
+    for (int off = 1; off < CH; off <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (!ok) return;
+    const int e = column_exponent(mx);
+    if (ch == 0) sa.ex[b * sa.n + c] = e;
+    split_chunk<T, NB>(sa, b, c - k1, ch, R, ldexp(1.0, 49 - e));
 }
 
 // ------------------------------------------------------- FP64 trailing update
@@ -391,12 +422,16 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         rec(tm ? tm->panel_events : nullptr, 2 * panel_idx);
-        if (cudaLaunchKernelEx(&cfg, pk, W, n, k0, st, piv, sa) != cudaSuccess) return PFB_ERR_CUDA;
+        if (cudaLaunchKernelEx(&cfg, pk, W, n, k0, st, piv) != cudaSuccess) return PFB_ERR_CUDA;
         rec(tm ? tm->panel_events : nullptr, 2 * panel_idx + 1);
 
         if (mt > 0) {
             rec(tm ? tm->update_events : nullptr, 2 * panel_idx);
             if (use_split) {
+                constexpr int cpb = 256 / (NB / 16);
+                split_slice_kernel<T, NB><<<dim3((unsigned)((mt + cpb - 1) / cpb), (unsigned)B), 256, 0, s>>>(
+                    W, n, k0, st, sa);
+                if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
                 int rc = launch_split_update(cplx, W, n, k0, K, B, st, sa, s);
                 if (rc != PFB_OK) return rc;
             } else {

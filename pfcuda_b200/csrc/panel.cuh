@@ -7,7 +7,6 @@
 
 #include "common.cuh"
 #include "large.cuh"
-#include "split.cuh"
 
 namespace pfb {
 
@@ -239,7 +238,7 @@ PFB_D c128 ld_remote(uint32_t addr, c128 *)
 // as clusters of one CTA (the ragged kernel), the barrier is bar.sync.
 template <typename T, int NB, int CPT, bool SOLO = false>
 PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, MatState *__restrict__ st,
-                      int32_t *__restrict__ piv, const SplitArgs &split, int64_t b)
+                      int32_t *__restrict__ piv)
 {
     using Real = typename RealOf<T>::type;
     using SM = PanelSmem<T, NB>;
@@ -527,13 +526,6 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         }
     if (has_panel && rank == 0 && pc < n) {
         for (int r = 0; r < NB && r < tid; r++) W[(int64_t)(k0 + r) * n + pc] = sm.lb[r][tid];
-    }
-    // the int8 operands of the split update; trailing columns exist only when
-    // the panel is full (t == NB/2), where the window is back in row order
-    if (split.enabled && t == NB / 2) {
-#pragma unroll
-        for (int q = 0; q < CPT; q++)
-            if (cq[q] < n) split_panel_column<T, NB>(split, b, cq[q] - k1, Rw[q], NB);
     }
     if (leader) {
         // keep the phase on the unit circle across panels

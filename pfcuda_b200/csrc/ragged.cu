@@ -219,7 +219,6 @@ ragged_kernel(const void *const *__restrict__ As, const int32_t *__restrict__ ns
     MatState *st = reinterpret_cast<MatState *>(mine + L.st_off);
     int32_t *piv = reinterpret_cast<int32_t *>(mine + L.piv_off);
     const int tid = threadIdx.x;
-    SplitArgs nosplit{};
 
     for (;;) {
         if (tid == 0) {
@@ -253,7 +252,7 @@ ragged_kernel(const void *const *__restrict__ As, const int32_t *__restrict__ ns
         }
         __syncthreads();
         for (int k0 = 0; k0 < n - 1; k0 += NB) {
-            panel_body<double, NB, kRaggedCPT, true>(sm.panel, W, n, k0, st, piv, nosplit, 0);
+            panel_body<double, NB, kRaggedCPT, true>(sm.panel, W, n, k0, st, piv);
             if (st->dead) break;
             const int K = (n - k0 < NB) ? n - k0 : NB;
             cta_update<NB, RaggedCfg<NB>::kUpdBlock>(W, n, k0, K, sm.strip);

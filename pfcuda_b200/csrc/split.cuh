@@ -75,83 +75,88 @@ PFB_D int8_t digit_of(long long x, int s)
     return (int8_t)(x < 0 ? -d : d);
 }
 
-// Slice one trailing column's K panel values into `slices` int8 digits with a
-// shared power-of-two scale (Ozaki's error-free splitting): with e the exponent
-// of the column's largest magnitude, every value x becomes
-// X = trunc(x 2^(49-e)) (|X| < 2^49, exact: a power-of-two scaling and a
-// truncation), and digit s is bits 42-7s .. 48-7s of |X| with x's sign -- the
-// same digits as repeated "multiply by 128, truncate, keep the remainder".
+// Ozaki's error-free splitting of one trailing column of the panel rows into
+// `slices` int8 digits under a shared power-of-two scale: with e the exponent
+// of the column's largest magnitude (column_exponent; mx < 2^e), every value x
+// becomes X = trunc(x 2^(49-e)) (|X| < 2^49, exact: a power-of-two scaling and
+// a truncation), and digit s is bits 42-7s .. 48-7s of |X| with x's sign --
+// the same digits as repeated "multiply by 128, truncate, keep the remainder".
 // Y's digits are X's with each (u, w) pair mapped to (w, -u).
-template <typename T, int NB>
-PFB_D void split_panel_column(const SplitArgs &sa, int64_t b, int col_rel, T (&R)[NB], int K)
+template <typename T>
+PFB_D double max_component(const T (&R)[16])
 {
-    if (!sa.enabled) return;
-    const int a = sa.k0 + sa.nb + col_rel;   // absolute trailing index
     double mx = 0.0;
 #pragma unroll
-    for (int r = 0; r < NB; r++) {
-        if (r >= K) R[r] = zero<T>();
+    for (int r = 0; r < 16; r++) {
         if constexpr (IsComplex<T>::value) mx = fmax(mx, fmax(fabs(R[r].re), fabs(R[r].im)));
         else mx = fmax(mx, fabs(R[r]));
     }
+    return mx;
+}
+
+PFB_D int column_exponent(double mx)
+{
     int e = 0;
-    if (mx > 0.0) frexp(mx, &e);          // mx < 2^e
-    sa.ex[b * sa.n + a] = e;
-    const double sc = ldexp(1.0, 49 - e);
+    if (mx > 0.0) frexp(mx, &e);
+    return e;
+}
+
+// Digits of rows 16 kc .. 16 kc + 15 of one column (R, scaled by sc = 2^(49-e))
+// into the A image (and the B images) of the split update.
+template <typename T, int NB>
+PFB_D void split_chunk(const SplitArgs &sa, int64_t b, int col_rel, int kc, const T (&R)[16], double sc)
+{
+    if constexpr (!IsComplex<T>::value) {
+        long long X[16];
 #pragma unroll
-    for (int kc = 0; kc < NB / 16; kc++) {
-        if constexpr (!IsComplex<T>::value) {
-            long long X[16];
+        for (int r = 0; r < 16; r++) X[r] = trunc_to_int(R[r] * sc);
+        for (int s = 0; s < sa.slices; s++) {
+            alignas(16) int8_t dx[16];
+            alignas(16) int8_t dy[16];
 #pragma unroll
-            for (int r = 0; r < 16; r++) X[r] = trunc_to_int(R[16 * kc + r] * sc);
-            for (int s = 0; s < sa.slices; s++) {
-                alignas(16) int8_t dx[16];
-                alignas(16) int8_t dy[16];
+            for (int r = 0; r < 16; r++) dx[r] = digit_of(X[r], s);
 #pragma unroll
-                for (int r = 0; r < 16; r++) dx[r] = digit_of(X[r], s);
-#pragma unroll
-                for (int r = 0; r < 16; r += 2) {   // (u, w) -> (w, -u)
-                    dy[r] = dx[r + 1];
-                    dy[r + 1] = (int8_t)(-dx[r]);
-                }
-                split_store16(sa.xs, sa, b, s, col_rel, kc, dx);
-                split_store16(sa.ys, sa, b, s, col_rel, kc, dy);
+            for (int r = 0; r < 16; r += 2) {   // (u, w) -> (w, -u)
+                dy[r] = dx[r + 1];
+                dy[r + 1] = (int8_t)(-dx[r]);
             }
-        } else {
-            // A = [Xr | Xi],  B1 = [Yr | -Yi],  B2 = [Yi | Yr]:  Re = A.B1, Im = A.B2
-            long long Xr[16], Xi[16];
+            split_store16(sa.xs, sa, b, s, col_rel, kc, dx);
+            split_store16(sa.ys, sa, b, s, col_rel, kc, dy);
+        }
+    } else {
+        // A = [Xr | Xi],  B1 = [Yr | -Yi],  B2 = [Yi | Yr]:  Re = A.B1, Im = A.B2
+        long long Xr[16], Xi[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            Xr[r] = trunc_to_int(R[r].re * sc);
+            Xi[r] = trunc_to_int(R[r].im * sc);
+        }
+        for (int s = 0; s < sa.slices; s++) {
+            alignas(16) int8_t xr[16];
+            alignas(16) int8_t xi[16];
+            alignas(16) int8_t yr[16];
+            alignas(16) int8_t yi[16];
+            alignas(16) int8_t t[16];
 #pragma unroll
             for (int r = 0; r < 16; r++) {
-                Xr[r] = trunc_to_int(R[16 * kc + r].re * sc);
-                Xi[r] = trunc_to_int(R[16 * kc + r].im * sc);
+                xr[r] = digit_of(Xr[r], s);
+                xi[r] = digit_of(Xi[r], s);
             }
-            for (int s = 0; s < sa.slices; s++) {
-                alignas(16) int8_t xr[16];
-                alignas(16) int8_t xi[16];
-                alignas(16) int8_t yr[16];
-                alignas(16) int8_t yi[16];
-                alignas(16) int8_t t[16];
 #pragma unroll
-                for (int r = 0; r < 16; r++) {
-                    xr[r] = digit_of(Xr[r], s);
-                    xi[r] = digit_of(Xi[r], s);
-                }
-#pragma unroll
-                for (int r = 0; r < 16; r += 2) {
-                    yr[r] = xr[r + 1];
-                    yr[r + 1] = (int8_t)(-xr[r]);
-                    yi[r] = xi[r + 1];
-                    yi[r + 1] = (int8_t)(-xi[r]);
-                }
-                split_store16(sa.xs, sa, b, s, col_rel, kc, xr);
-                split_store16(sa.xs, sa, b, s, col_rel, NB / 16 + kc, xi);
-                split_store16(sa.ys, sa, b, s, col_rel, kc, yr);
-#pragma unroll
-                for (int r = 0; r < 16; r++) t[r] = (int8_t)(-yi[r]);
-                split_store16(sa.ys, sa, b, s, col_rel, NB / 16 + kc, t);
-                split_store16(sa.ys2, sa, b, s, col_rel, kc, yi);
-                split_store16(sa.ys2, sa, b, s, col_rel, NB / 16 + kc, yr);
+            for (int r = 0; r < 16; r += 2) {
+                yr[r] = xr[r + 1];
+                yr[r + 1] = (int8_t)(-xr[r]);
+                yi[r] = xi[r + 1];
+                yi[r + 1] = (int8_t)(-xi[r]);
             }
+            split_store16(sa.xs, sa, b, s, col_rel, kc, xr);
+            split_store16(sa.xs, sa, b, s, col_rel, NB / 16 + kc, xi);
+            split_store16(sa.ys, sa, b, s, col_rel, kc, yr);
+#pragma unroll
+            for (int r = 0; r < 16; r++) t[r] = (int8_t)(-yi[r]);
+            split_store16(sa.ys, sa, b, s, col_rel, NB / 16 + kc, t);
+            split_store16(sa.ys2, sa, b, s, col_rel, kc, yi);
+            split_store16(sa.ys2, sa, b, s, col_rel, NB / 16 + kc, yr);
         }
     }
 }
