@@ -196,13 +196,13 @@ gemm_dmma_kernel(double *__restrict__ W_all, int n, int k0, int K, const MatStat
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Xs = reinterpret_cast<double *>(smem_raw);   // [KMAX][kDmmaLD]: rows k0.., columns a0..
     double *Ys = Xs + KMAX * kDmmaLD;                     // [KMAX][kDmmaLD]: rows k0.., columns b0..
-    const int64_t b = blockIdx.y;
+    const int64_t b = blockIdx.x;
     if (st_all[b].dead) return;
     double *W = W_all + b * (int64_t)n * n;
     const int k1 = k0 + K;
     const int nt = (n - k1 + kDmmaBM - 1) / kDmmaBM;
     int I, J;
-    upper_block(blockIdx.x, nt, I, J);
+    upper_block(nt * (nt + 1) / 2 - 1 - (int)blockIdx.y, nt, I, J);
     const int a0 = k1 + I * kDmmaBM, b0 = k1 + J * kDmmaBM;
     const bool diag = I == J;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -253,13 +253,13 @@ gemm_zdmma_kernel(c128 *__restrict__ W_all, int n, int k0, int K, const MatState
     extern __shared__ __align__(16) unsigned char smem_raw[];
     c128 *Xs = reinterpret_cast<c128 *>(smem_raw);   // [KMAX][kZdmmaLD]: rows k0.., columns a0..
     c128 *Ys = Xs + KMAX * kZdmmaLD;                  // [KMAX][kZdmmaLD]: rows k0.., columns b0..
-    const int64_t b = blockIdx.y;
+    const int64_t b = blockIdx.x;
     if (st_all[b].dead) return;
     c128 *W = W_all + b * (int64_t)n * n;
     const int k1 = k0 + K;
     const int nt = (n - k1 + kZdmmaBM - 1) / kZdmmaBM;
     int I, J;
-    upper_block(blockIdx.x, nt, I, J);
+    upper_block(nt * (nt + 1) / 2 - 1 - (int)blockIdx.y, nt, I, J);
     const int a0 = k1 + I * kZdmmaBM, b0 = k1 + J * kZdmmaBM;
     const bool diag = I == J;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -437,10 +437,13 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
             } else {
                 const int nt = (mt + BM - 1) / BM;
                 const unsigned tiles = (unsigned)(nt * (nt + 1) / 2);
+                // blockIdx.x = matrix, blockIdx.y = tile from the last: the blocks start in
+                // that order, so the first row tile (the next panel's rows) is written
+                // last and is still in L2 when the next panel loads it
                 if constexpr (cplx)
-                    gemm_zdmma_kernel<NB><<<dim3(tiles, (unsigned)B), 256, gsmem, s>>>(W, n, k0, K, st);
+                    gemm_zdmma_kernel<NB><<<dim3((unsigned)B, tiles), 256, gsmem, s>>>(W, n, k0, K, st);
                 else
-                    gemm_dmma_kernel<NB><<<dim3(tiles, (unsigned)B), kDmmaThreads, gsmem, s>>>(W, n, k0, K, st);
+                    gemm_dmma_kernel<NB><<<dim3((unsigned)B, tiles), kDmmaThreads, gsmem, s>>>(W, n, k0, K, st);
                 if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
             }
             rec(tm ? tm->update_events : nullptr, 2 * panel_idx + 1);

@@ -177,7 +177,10 @@ PFB_D void tmem_ld8(uint32_t taddr, int32_t (&v)[8])
 }
 
 // Upper-triangle tiles of the trailing block in row-major order: row tile I
-// (TM rows) holds column tiles J = I*R .. ntn-1, R = TM/TN.
+// (TM rows) holds column tiles J = I*R .. ntn-1, R = TM/TN.  A CTA walks its
+// range backwards (step): the first row tile, which holds the next panel's
+// rows, is then among the last tiles written and still in L2 when the next
+// panel kernel loads it.
 struct TileWalk {
     int ntn, R, I, J;
     PFB_D void start(int idx)
@@ -186,9 +189,9 @@ struct TileWalk {
         while (idx >= ntn - I * R) { idx -= ntn - I * R; I++; }
         J = I * R + idx;
     }
-    PFB_D void next()
+    PFB_D void step()
     {
-        if (++J >= ntn) { I++; J = I * R; }
+        if (--J < I * R) { I--; J = ntn - 1; }
     }
 };
 
@@ -357,9 +360,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
         if (lane == 0) {
             const int64_t chunk = (int64_t)TM * kk;
             TileWalk tw{ntn, R, 0, 0};
-            tw.start(t0);
+            tw.start(t1 - 1);
             int arow = -1, aloads = 0;
-            for (int it = 0; it < ntiles && ok; it++, tw.next()) {
+            for (int it = 0; it < ntiles && ok; it++, tw.step()) {
                 if (tw.I != arow) {
                     if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1);
                     if (!ok) break;
@@ -396,9 +399,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             const uint64_t adesc0 = smem_desc(su32(sA), 128, sbo);
             const uint64_t bdesc0 = smem_desc(su32(sB), 128, sbo);
             TileWalk tw{ntn, R, 0, 0};
-            tw.start(t0);
+            tw.start(t1 - 1);
             int arow = -1, aloads = 0;
-            for (int it = 0; it < ntiles && ok; it++, tw.next()) {
+            for (int it = 0; it < ntiles && ok; it++, tw.step()) {
                 if (tw.I != arow) {
                     if (aloads > 0) mma_commit(mb(1));          // A may be replaced once these MMAs finish
                     ok = mbar_wait_bounded(mb(0), aloads & 1);
@@ -440,7 +443,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
         const int r = quarter * 32 + lane;          // row within the tile
         const int bz = (int)b;
         TileWalk tw{ntn, R, 0, 0};
-        tw.start(t0);
+        tw.start(t1 - 1);
         TileWalk tl = tw;                           // the leader's load cursor, one tile ahead
         // (tile coordinates are passed by value: a reference would put the
         // cursors in local memory)
@@ -455,7 +458,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     } while (0)
         if (leader) {
             PFB_LOAD_C(0, tl.I, tl.J);
-            tl.next();
+            tl.step();
             if (ntiles > 1) PFB_LOAD_C(1, tl.I, tl.J);
         }
         for (int it = 0; it < ntiles && ok; it++) {
@@ -501,7 +504,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             if (leader && it >= 1 && it + 1 < ntiles) {
                 // the store of tile it-1 has long read its buffer: load tile it+1 there
                 bulk_wait_read0();
-                tl.next();
+                tl.step();
                 PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
             }
             // read-modify-write of the CW * NOUT doubles in shared memory:
@@ -536,7 +539,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
                     tma_store_3d(&cmap, x0 + q * kCBoxCols, y, bz, su32(cb + q * kCBoxBytes));
                 bulk_commit();
             }
-            tw.next();
+            tw.step();
         }
 #undef PFB_LOAD_C
         if (leader) bulk_wait0();
