@@ -54,3 +54,15 @@ def test_bad_inputs():
         pf.pfaffian(torch.zeros(3, 4))
     with pytest.raises(TypeError):
         pf.pfaffian(torch.zeros(8, 8, dtype=torch.int32))
+
+
+def test_mode_resolution():
+    assert pf.resolve_mode("auto", torch.float64) == "split"
+    assert pf.resolve_mode("auto", torch.float32) == "split"
+    assert pf.resolve_mode("auto", torch.complex128) == "fp64"
+    assert pf.resolve_mode("auto", torch.complex64) == "fp64"
+    assert pf.resolve_mode("fp64", torch.float64) == "fp64"
+    with pytest.raises(ValueError, match="mode"):
+        pf.resolve_mode("tf32", torch.float64)
+    with pytest.raises(ValueError, match="mode"):
+        pf.slog_pfaffian(torch.zeros(40, 40, dtype=torch.float64), mode="tf32")

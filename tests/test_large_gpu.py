@@ -190,3 +190,13 @@ def test_max_concurrent_query():
         assert m >= 1
     assert L.pfb_slog_max_concurrent(_lib.F64, 16) == 0          # small path
     assert L.pfb_slog_max_concurrent(_lib.F64, 1 << 20) == 0     # beyond the large path
+
+
+def test_auto_mode_picks_per_dtype():
+    """slog_pfaffian's default mode: split for real inputs, fp64 for complex."""
+    rng = np.random.default_rng(31)
+    for cplx, want in ((False, "split"), (True, "fp64")):
+        A = cuda(O.skew_normal(rng, 2, 130, scale=1 / np.sqrt(130), complex_=cplx))
+        la, sg = pf.slog_pfaffian(A)
+        lw, sw = pf.slog_pfaffian(A, mode=want)
+        assert torch.equal(la, lw) and torch.equal(sg, sw)
