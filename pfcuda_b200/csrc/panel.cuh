@@ -103,6 +103,7 @@ struct PanelSmem {
     static constexpr int NW = NT / 32;
     T lb[NB][NB + 1];                  // replicated NB x NB block of the panel columns
     alignas(16) T stage[2][NB];        // this CTA's best trailing column, panel rows 0..NB-1
+    T k1col[2][NB];                    // the entries a trailing pivot column takes in the interchange
     PivHdr<T> hdr[2][kClusterMax];     // per-CTA best candidate, pushed by every CTA of the cluster
     T wval[NW];                        // per-warp best candidate
     unsigned long long wkey[NW];       // its key as bits
@@ -354,6 +355,15 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                 store_pair(&sm.stage[par][r], v0, v1);
             }
         }
+        // if the pivot column is a trailing one, its owner fills its window
+        // from column k+1 of the panel rows above k+1 and the negated row k+1
+        // right of it: saved here, so that (5) can overwrite them in lb
+        // without a barrier between the owner's reads and those writes
+        if (has_panel) {
+            const int x = tid;
+            sm.k1col[par][x] = (x <= 2 * t) ? sm.lb[x][2 * t + 1]
+                                            : ((x > 2 * t + 1) ? neg(sm.lb[2 * t + 1][x]) : zero<T>());
+        }
         group_sync<SOLO>();
 
         // (4) the pivot: the first maximum over the CL <= 16 headers, lane s of
@@ -410,8 +420,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                         for (int p = 0; p < NB; p++) {
                             const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
                             if (p == 1) Rw[q][1] = neg(Rw[q][1]);
-                            else if (r <= 2 * t) Rw[q][p] = sm.lb[r][2 * t + 1];
-                            else Rw[q][p] = neg(sm.lb[2 * t + 1][r]);
+                            else Rw[q][p] = sm.k1col[par][r];
                         }
                     } else if (c < n) {
                         // the old row k+1 entry goes to this slot in (6), after the
@@ -426,7 +435,9 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                 if (has_panel)
                     tJ = ld_remote(map_rank(smem_u32(&sm.stage[par][tid]), (uint32_t)gs), (T *)nullptr);
             }
-            __syncthreads();
+            // no barrier here: every lb entry below is read above by the thread
+            // that writes it (panel thread x reads and writes only lb[x][.] and
+            // lb[.][x]), and the trailing owner of column j read k1col instead
             if (has_panel) {
                 const int x = tid;
                 if (!trail_win) {
