@@ -154,7 +154,8 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"slog_pfaffian 2n={n} float64, seed 1", "n": n, "batch": 1},
+        "config": {"workload": f"slog_pfaffian of independent 2n={n} float64 matrices, seed 1 (+rank)",
+                   "n": n, "batch": threads},
         "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -660,8 +661,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if tdt == torch.float64 else "c128",
         "data": "synthetic",
-        "config": {"workload": f"slog_pfaffian of independent 2n={n} {args.dtype} matrices, seed 1 (+rank), "
-                               f"{B} per call", "n": n, "batch": B, "mode": head, "panel_width": nb,
+        "config": {"workload": f"slog_pfaffian of independent 2n={n} {args.dtype} matrices, seed 1 (+rank)",
+                   "n": n, "batch": B, "mode": head, "panel_width": nb,
                    "l2": f"inputs {B * n * n * esz / 1e6:.0f} MB > 126 MB L2, re-read every step",
                    "parallelism": f"replicas x{world}"},
         "modes_ms_per_step": results,
