@@ -15,9 +15,9 @@
 //     w = -(updated row k+1) (apply_updates, slog_pfaffian_lg.cu:136-149), so the
 //     Schur complement is S = A22 + sum (u w^T - w u^T).
 // The shape is new and runs entirely on the device:
-//   * copy_in: the input (any dtype, either layout) becomes an FP64 / complex128
-//     working matrix W in the workspace, row-major, of which only the strict
-//     upper triangle is read from then on.
+//   * copy_in: the upper triangle of the input's row-major view (any dtype,
+//     either layout) becomes an FP64 / complex128 working matrix W in the
+//     workspace; nothing reads below its diagonal.
 //   * panel_kernel (one thread-block cluster per matrix): NB pivot rows at a
 //     time.  Each trailing column of the panel rows lives in the registers of
 //     one thread, the NB x NB block of panel columns is replicated in every
@@ -109,13 +109,23 @@ size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode)
 
 // ----------------------------------------------------------------- copy in
 
+// W <- A widened, the upper triangle only (diagonal included): nothing reads
+// below the diagonal of W.  One warp per row at a time, the row's columns
+// r .. n-1 in coalesced runs of 32.
 template <typename S, typename T>
-__global__ void copy_in_kernel(const S *__restrict__ A, T *__restrict__ W, int64_t total,
-                               MatState *st, int64_t batch)
+__global__ void copy_in_kernel(const S *__restrict__ A, T *__restrict__ W, int64_t batch, int n,
+                               MatState *st)
 {
+    const int lane = threadIdx.x & 31;
+    const int64_t rows = batch * n;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t R = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; R < rows; R += nwarps) {
+        const int r = (int)(R % n);
+        const S *src = A + R * n;
+        T *dst = W + R * n;
+        for (int c = r + lane; c < n; c += 32) dst[c] = conv<T>(src[c]);
+    }
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride)
-        W[e] = conv<T>(A[e]);
     for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += stride) {
         MatState s;
         s.log_abs = 0.0;
@@ -336,31 +346,26 @@ static int run_large(const void *A, int dtype, int64_t B, int n, int layout, int
     int32_t *piv = reinterpret_cast<int32_t *>(ws + L.piv_off);
     MatState *st = reinterpret_cast<MatState *>(ws + L.st_off);
     T *W = reinterpret_cast<T *>(ws + L.w_off);
-    const int64_t total = B * (int64_t)n * n;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
     {
-        int64_t blocks = (total + 255) / 256;
+        int64_t blocks = (B * (int64_t)n + 7) / 8;   // 8 warps (rows) per block
         if (blocks > (int64_t)sms * 16) blocks = (int64_t)sms * 16;
         if (blocks < 1) blocks = 1;
         switch (dtype) {
         case PFB_F32:
-            copy_in_kernel<float, double><<<(unsigned)blocks, 256, 0, s>>>(
-                (const float *)A, (double *)W, total, st, B);
+            copy_in_kernel<float, double><<<(unsigned)blocks, 256, 0, s>>>((const float *)A, (double *)W, B, n, st);
             break;
         case PFB_F64:
-            copy_in_kernel<double, double><<<(unsigned)blocks, 256, 0, s>>>(
-                (const double *)A, (double *)W, total, st, B);
+            copy_in_kernel<double, double><<<(unsigned)blocks, 256, 0, s>>>((const double *)A, (double *)W, B, n, st);
             break;
         case PFB_C64:
-            copy_in_kernel<c64, c128><<<(unsigned)blocks, 256, 0, s>>>(
-                (const c64 *)A, (c128 *)W, total, st, B);
+            copy_in_kernel<c64, c128><<<(unsigned)blocks, 256, 0, s>>>((const c64 *)A, (c128 *)W, B, n, st);
             break;
         default:
-            copy_in_kernel<c128, c128><<<(unsigned)blocks, 256, 0, s>>>(
-                (const c128 *)A, (c128 *)W, total, st, B);
+            copy_in_kernel<c128, c128><<<(unsigned)blocks, 256, 0, s>>>((const c128 *)A, (c128 *)W, B, n, st);
             break;
         }
         if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;

@@ -170,3 +170,17 @@ def test_autograd_pfaffian_small():
         if cplx:
             want = want.conj()
         assert np.all(rel(At.grad.cpu().numpy(), want) <= bound(A))
+
+
+def test_grad_ignores_lower_triangle():
+    """The adjoint, like the forward pass, reads only the upper triangle of
+    the input's row-major view: NaN below the diagonal changes nothing."""
+    rng = np.random.default_rng(14)
+    for cplx in (False, True):
+        A = O.skew_normal(rng, 2, 130, scale=1 / np.sqrt(130), complex_=cplx)
+        D = A.copy()
+        il = np.tril_indices(130, -1)
+        D[:, il[0], il[1]] = np.nan
+        G1, l1, s1 = run(A)
+        G2, l2, s2 = run(D)
+        assert np.array_equal(G1, G2) and np.array_equal(l1, l2) and np.array_equal(s1, s2)
