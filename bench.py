@@ -653,8 +653,9 @@ def main():
         roof = {"kernel": kname, "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic_ratio[kname] * upd_bytes / max(npan - 1, 1),
-                "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch; "
-                        "traffic per launch scaled from ncu"}
+                "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch; the "
+                        "timed region includes the operand-slicing launch before each update; traffic per "
+                        "launch scaled from ncu"}
     roof["peak_source"] = "MEASURED_PEAKS.json hbm_gbs (measured)"
     line = {
         "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
