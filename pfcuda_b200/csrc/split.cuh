@@ -40,6 +40,16 @@ struct SplitArgs {
 size_t split_workspace_bytes(bool cplx, int64_t batch, int n, int nb);
 SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int n, int nb, int k0,
                      int slices);
+// The same arrays seen from matrix b0 on (a range of the batch).
+inline SplitArgs split_shift(SplitArgs a, int64_t b0)
+{
+    a.xs += b0 * a.mstride;
+    a.ys += b0 * a.mstride;
+    if (a.ys2) a.ys2 += b0 * a.mstride;
+    a.ex += b0 * (int64_t)a.n;
+    a.err += b0;
+    return a;
+}
 bool split_available();
 int launch_split_update(bool cplx, void *W, int n, int k0, int K, int64_t batch,
                         MatState *st, const SplitArgs &sa, cudaStream_t stream);
