@@ -623,6 +623,13 @@ def main():
 
     ms = results[head]
     value = world * B / (ms * 1e-3)
+    # kernel launches per call: the library runs a batch of three or more waves
+    # of the widest panel clusters (9 or more CTAs) as two ranges, each with
+    # its own sequence of launches
+    cpt = 1 if (nb == 64 or tdt == torch.complex128) else 2
+    widest = (n - nb + 256 * cpt - 1) // (256 * cpt)
+    mc = int(L.pfb_slog_max_concurrent(dtc, n))
+    ranges = 2 if (widest >= 9 and mc > 0 and B >= 3 * mc) else 1
     esz = A.element_size()
     hbm_peak = _hbm_peak()
     # trailing update, the kernel that carries the O(n^3) arithmetic: each of
@@ -681,7 +688,7 @@ def main():
                        "slog_pfaffian_raw and the results back to pinned host memory; two device buffers "
                        "so the upload of step i+1 overlaps the factorisation of step i",
                 "results_equal_device_path": e2e_same},
-        "gpu_launches": args.steps * (2 + npan + (npan - 1) * (2 if head == "split" else 1)),
+        "gpu_launches": args.steps * ranges * (2 + npan + (npan - 1) * (2 if head == "split" else 1)),
         "clocks": clocks,
     }
     if world == 1:
