@@ -4,11 +4,14 @@
  * Plain C types only: device pointers, sizes, enums and a cudaStream_t passed as
  * void*.  Every entry point
  *   - enqueues its work on `stream` and returns without synchronising the host,
- *   - allocates nothing: scratch memory is the caller's `workspace`, whose size
- *     the matching *_workspace_bytes function gives,
+ *   - allocates no device memory: scratch memory is the caller's `workspace`,
+ *     whose size the matching *_workspace_bytes function gives (the one
+ *     exception, pfb_slog_pfaffian_noalloc, says how it differs),
  *   - never throws and never writes its input; errors come back as a pfb_status,
- *   - is re-entrant (no global mutable state), so several streams or threads may
- *     call it at once.
+ *   - is re-entrant, so several streams or threads may call it at once: the only
+ *     state kept between calls is read-only after its first use (device
+ *     properties, the split kernel's tensor-map entry point) or private to the
+ *     calling host thread (the second stream of pfb_slog_stream_ranges).
  *
  * Matrices are batches of `batch` contiguous n x n arrays.  `layout` says how one
  * matrix is stored: PFB_ROW_MAJOR (C order, torch/NumPy default) or PFB_COL_MAJOR
@@ -53,6 +56,13 @@ typedef enum {
  * digits per operand (1..7; 0 selects the default, 7).  Fewer digits trade
  * accuracy for speed: S digits keep the update to about K * 2^(-7S) relative. */
 #define PFB_SPLIT_DIGITS(s) ((s) << 8)
+/* Test only, PFB_MODE_SPLIT: every bounded device-side wait of the split
+ * update's pipeline for the first matrix of the call gives up without polling,
+ * exactly as a wait that ran out of its bound would.  That matrix's result is
+ * log = NaN, sign = 0 (the update kernel lets its copies and MMAs in flight land
+ * and frees its tensor memory before it returns); the other matrices of the
+ * call are unaffected and the device stays usable. */
+#define PFB_SPLIT_TEST_TIMEOUT (1 << 12)
 
 typedef enum {
     PFB_OK = 0,
@@ -139,6 +149,20 @@ int pfb_slog_panel_width(int dtype, int n);
 int pfb_slog_max_concurrent(int dtype, int n);
 
 /*
+ * How many ranges a pfb_slog_pfaffian call on `batch` matrices of order n runs
+ * as (1 or 2).  A batch of three or more waves of the widest panel clusters
+ * (clusters of 9 or more CTAs) is split in two: the last wave's worth of
+ * matrices runs on a second stream that forks from and joins `stream` through
+ * events, so its trailing updates fill the SMs the first range's panel waves
+ * leave idle.  The second stream belongs to the calling host thread (one per
+ * thread and device, created on its first use and destroyed when the thread
+ * exits), so calls from different threads never share it; a call whose
+ * thread's second stream is part of another graph capture runs as one range.
+ * Each range launches its own sequence of kernels.  No reference counterpart.
+ */
+int pfb_slog_stream_ranges(int dtype, int64_t batch, int n);
+
+/*
  * (log|Pf|, sign) of a ragged batch in one launch: `count` matrices of even (or
  * odd) orders n[i] <= max_n <= PFB_RAGGED_MAX_N, each float32 or float64
  * (dtype[i]), each contiguous at A[i] in `layout`.  A, n and dtype are DEVICE
@@ -180,8 +204,10 @@ int pfb_slog_pivots(int64_t batch, int n, const void *workspace, size_t workspac
  *     PFB_NOALLOC_SCRATCH_BYTES return PFB_ERR_SIZE (n <= 32 needs no scratch);
  *     e.g. one float64 matrix fits up to n = 1448 (1392 in PFB_MODE_SPLIT), one
  *     complex128 matrix up to n = 1022 (980 in PFB_MODE_SPLIT).
- *   - The first call on a device looks up the array's device address; make that
- *     first call before any stream capture.
+ *   - Every call looks up the array's device address on the current device
+ *     (nothing is cached, so a device reset between calls is harmless); the
+ *     first call on a device also loads the library's module there, so make
+ *     that first call before any stream capture.
  *   - All calls share the array: calls that overlap on the GPU race and must be
  *     serialised by the caller.
  * Nothing is allocated; arguments and results are those of pfb_slog_pfaffian.
@@ -203,8 +229,16 @@ int pfb_slog_pfaffian_noalloc(int dtype, const void *A, int64_t batch, int n, in
  *   log_out / sign_out: the forward results, exactly as pfb_slog_pfaffian;
  *   a matrix with Pf = 0 gets an all-NaN gradient.
  * n must be even (odd orders have Pf = 0 identically: PFB_ERR_SIZE) and within
- * the large path's range.  workspace: pfb_slog_grad_workspace_bytes bytes,
- * 256-aligned (about 3 n^2 elements of the working type per matrix).
+ * the large path's range.
+ * workspace (256-aligned) is the call's memory budget: about 2 n^2 elements of
+ * the working type per matrix (the factors and the inverse of their unit
+ * triangle), pfb_slog_grad_workspace_bytes(dtype, batch, n, mode) for the whole
+ * batch at once.  Any smaller workspace of at least
+ * pfb_slog_grad_workspace_bytes(dtype, 1, n, mode) bytes is accepted: the batch
+ * then runs in chunks of as many matrices as fit, each chunk's factors formed,
+ * used and overwritten by the next chunk's.  Results do not depend on the
+ * chunking (every matrix's arithmetic is its own).  The reference's rule keeps
+ * no factors but calls a general inverse per matrix (cuda_api.py:84-89).
  */
 int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                            const double *ct_log, void *G_out, double *log_out, void *sign_out,

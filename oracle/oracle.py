@@ -256,16 +256,17 @@ def haar_orthogonal(rng, n):
     return Q * np.sign(np.diag(R))
 
 
-def config_illcond(seed=4, B=64, n=2048, dtype=np.float64):
+def config_illcond(seed=4, B=64, n=2048, dtype=np.float64, return_q=False):
     """A = Q blockdiag(s_k J) Q^T, s_k log-spaced in [1e-6, 1]; returns (A, exact
-    log|Pf| = sum log s_k, exact sign = det Q) per matrix."""
+    log|Pf| = sum log s_k, exact sign = det Q) per matrix, and with ``return_q``
+    the Haar factors Q as well (for the exact inverse, illcond_half_inv_t)."""
     rng = np.random.default_rng(seed)
     s = np.logspace(-6, 0, n // 2)
     D = np.zeros((n, n))
     idx = np.arange(0, n, 2)
     D[idx, idx + 1] = s
     D[idx + 1, idx] = -s
-    As, logs, signs = [], [], []
+    As, logs, signs, Qs = [], [], [], []
     for _ in range(B):
         Q = haar_orthogonal(rng, n)
         A = Q @ D @ Q.T
@@ -273,7 +274,25 @@ def config_illcond(seed=4, B=64, n=2048, dtype=np.float64):
         As.append(A.astype(dtype))
         logs.append(np.sum(np.log(s)))
         signs.append(np.sign(np.linalg.det(Q)))
-    return np.stack(As), np.array(logs), np.array(signs)
+        if return_q:
+            Qs.append(Q)
+    out = (np.stack(As), np.array(logs), np.array(signs))
+    return out + (np.stack(Qs),) if return_q else out
+
+
+def illcond_half_inv_t(Q):
+    """The exact d log Pf / dA = (1/2) A^-T of config_illcond's construction:
+    A^-1 = Q blockdiag(-J / s_k) Q^T (J^-1 = -J), so (1/2) A^-T = -(1/2) A^-1 =
+    (1/2) Q blockdiag(J / s_k) Q^T, formed in float64 from the stored Q."""
+    Q = np.asarray(Q, dtype=np.float64)
+    n = Q.shape[-1]
+    s = np.logspace(-6, 0, n // 2)
+    idx = np.arange(0, n, 2)
+    # Q blockdiag(J / s) Q^T = sum_k (q_2k q_2k+1^T - q_2k+1 q_2k^T) / s_k
+    Qe = Q[..., :, idx] / s
+    Qo = Q[..., :, idx + 1]
+    M = Qe @ np.swapaxes(Qo, -1, -2)
+    return 0.5 * (M - np.swapaxes(M, -1, -2))
 
 
 def tridiag_known(rng, n):

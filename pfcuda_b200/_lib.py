@@ -32,6 +32,7 @@ SIGNATURES = {
     "pfb_slog_pfaffian_timed": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _sz, _vp, _vp]),
     "pfb_slog_panel_width": (_int, [_int, _int]),
     "pfb_slog_max_concurrent": (_int, [_int, _int]),
+    "pfb_slog_stream_ranges": (_int, [_int, _i64, _int]),
     "pfb_slog_pfaffian_ragged": (_int, [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp, _sz, _vp]),
     "pfb_slog_ragged_workspace_bytes": (_sz, [_i64, _int]),
     "pfb_slog_pfaffian_noalloc": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp]),

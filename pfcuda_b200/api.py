@@ -250,43 +250,118 @@ def slog_pfaffian_ragged(mats, layout: int = _lib.ROW_MAJOR):
 
 
 # ------------------------------------------------------------- autograd glue
+#
+# The reference differentiates with forward-mode rules (jax.custom_jvp,
+# pfcuda/cuda_api.py:78-107):
+#     d log Pf = (1/2) tr(A^-1 dA),   d Pf = Pf * (1/2) tr(A^-1 dA),
+# each evaluated with a general inverse (jnp.linalg.inv).  Here both modes run
+# through the engine's adjoint kernel, which forms G = (1/2) A^-T from the
+# blocked factors (pfcuda_b200.grad); tr(A^-1 dA)/2 is then sum_ij G_ij dA_ij.
+# For complex A, log|Pf| = Re(log Pf) and the phase s = Pf/|Pf| = exp(i Im
+# log Pf), so d log|Pf| = Re(t) and d s = s * i Im(t) with t = sum G * dA (the
+# reference returns a zero sign tangent, which is exact only for real input).
+# torch's backward convention for complex tensors is the conjugate Wirtinger
+# derivative: a real cotangent g of log|Pf| gives g * conj(G), and a cotangent
+# h of the phase adds i Im(h conj(s)) * conj(G).
 
-class _PfaffianFn(torch.autograd.Function):
+
+class _Adjoint(torch.autograd.Function):
+    """ct * (1/2) A^-T through the engine's adjoint kernel, as an operation that
+    torch's transforms (torch.func.jvp / vjp / grad) can call: they hand its
+    forward plain tensors, whose data pointers the C ABI needs.  Its own
+    derivatives (second derivatives of log Pf) are not provided."""
+
     @staticmethod
-    def forward(ctx, A):
-        pf = pfaffian_raw(A)
-        ctx.save_for_backward(A, pf)
-        return pf
+    def forward(A, ct, mode):
+        from .grad import slog_pfaffian_grad
+        return slog_pfaffian_grad(A, ct=ct, mode=mode)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        pass
 
     @staticmethod
     def backward(ctx, g):
-        # d Pf = (1/2) Pf tr(A^-1 dA)  (pfcuda/cuda_api.py:85-97), so
-        # dPf/dA = Pf * (1/2) A^-T, with (1/2) A^-T from the engine's adjoint
-        # kernel; torch wants the conjugate for complex A.
-        from .grad import slog_pfaffian_grad
+        raise NotImplementedError("second derivatives of slog_pfaffian / pfaffian are not provided")
+
+    @staticmethod
+    def jvp(ctx, dA, dct, dmode):
+        raise NotImplementedError("second derivatives of slog_pfaffian / pfaffian are not provided")
+
+
+def _half_inv_t(A, mode="fp64", ct=None):
+    return _Adjoint.apply(A, ct, mode)
+
+
+def _contract(G, dA):
+    """sum_ij G_ij dA_ij per matrix (no conjugation): (1/2) tr(A^-1 dA)."""
+    return (G * dA.to(G.dtype)).sum(dim=(-2, -1))
+
+
+class _PfaffianFn(torch.autograd.Function):
+    @staticmethod
+    def forward(A):
+        return pfaffian_raw(A)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        (A,) = inputs
+        ctx.save_for_backward(A, output)
+        ctx.save_for_forward(A, output)
+
+    @staticmethod
+    def backward(ctx, g):
+        # dPf/dA = Pf * (1/2) A^-T (pfcuda/cuda_api.py:78-90); torch wants the
+        # conjugate for complex A.
         A, pf = ctx.saved_tensors
-        G = slog_pfaffian_grad(A, mode="fp64")
+        G = _half_inv_t(A)
         if A.is_complex():
             G = G.conj()
             pf = pf.conj()
         return (g * pf)[..., None, None] * G
 
+    @staticmethod
+    def jvp(ctx, dA):
+        # d Pf = Pf * (1/2) tr(A^-1 dA)  (pfcuda/cuda_api.py:78-90)
+        A, pf = ctx.saved_tensors
+        return pf * _contract(_half_inv_t(A), dA).to(pf.dtype)
+
 
 class _SlogFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, A, mode):
-        la, sg = slog_pfaffian_raw(A, mode)
-        ctx.save_for_backward(A)
+    def forward(A, mode):
+        return slog_pfaffian_raw(A, mode)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        A, mode = inputs
+        la, sg = output
         ctx.mode = mode
-        ctx.mark_non_differentiable(sg)
-        return la, sg
+        ctx.save_for_backward(A, sg)
+        ctx.save_for_forward(A, sg)
+        if not A.is_complex():
+            ctx.mark_non_differentiable(sg)   # +-1: piecewise constant
 
     @staticmethod
     def backward(ctx, g_log, g_sign):
-        # d log Pf = (1/2) tr(A^-1 dA)  (pfcuda/cuda_api.py:92-107); the engine
-        # returns g * (1/2) A^-T with the cotangent applied in its last kernel.
-        # torch's convention for a real function of complex A is the conjugate.
-        from .grad import slog_pfaffian_grad
-        (A,) = ctx.saved_tensors
-        G = slog_pfaffian_grad(A, ct=g_log, mode=ctx.mode)
-        return (G.conj() if A.is_complex() else G), None
+        # d log|Pf| / dA = (1/2) A^-T  (pfcuda/cuda_api.py:92-107); for real A
+        # the engine applies the cotangent in its last kernel.
+        A, sg = ctx.saved_tensors
+        if not A.is_complex():
+            return _half_inv_t(A, ctx.mode, ct=g_log), None
+        c = torch.zeros(A.shape[:-2], dtype=A.dtype, device=A.device)
+        if g_log is not None:
+            c = c + g_log.to(A.dtype)
+        if g_sign is not None:
+            c = c + 1j * (g_sign * sg.conj()).imag.to(A.dtype)
+        return c[..., None, None] * _half_inv_t(A, ctx.mode).conj(), None
+
+    @staticmethod
+    def jvp(ctx, dA, _dmode):
+        # d log|Pf| = Re (1/2) tr(A^-1 dA)  (pfcuda/cuda_api.py:92-107); the
+        # phase of complex A turns by i Im of the same trace.
+        A, sg = ctx.saved_tensors
+        t = _contract(_half_inv_t(A, ctx.mode), dA)
+        if A.is_complex():
+            return t.real.to(torch.float64), sg * (1j * t.imag).to(sg.dtype)
+        return t.to(torch.float64), None   # the sign of real A is piecewise constant

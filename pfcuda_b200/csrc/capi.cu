@@ -77,6 +77,12 @@ int pfb_slog_max_concurrent(int dtype, int n)
     return pfb::large_max_concurrent(dtype, n);
 }
 
+int pfb_slog_stream_ranges(int dtype, int64_t batch, int n)
+{
+    if (!valid_dtype(dtype) || batch <= 0 || n <= 32 || (n & 1)) return 1;
+    return pfb::large_second_range(dtype, batch, n) > 0 ? 2 : 1;
+}
+
 int pfb_slog_panel_width(int dtype, int n)
 {
     if (!valid_dtype(dtype) || n < 0) return 0;
@@ -89,7 +95,7 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
 {
     if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
     if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
-    if ((mode & ~0xfff) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
+    if ((mode & ~(0xfff | PFB_SPLIT_TEST_TIMEOUT)) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
     if (batch == 0) return PFB_OK;
     if (!log_out || !sign_out || (!A && n > 0)) return PFB_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
@@ -121,15 +127,15 @@ int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int l
 {
     if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
     if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
-    if ((mode & ~0xfff) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
+    if ((mode & ~(0xfff | PFB_SPLIT_TEST_TIMEOUT)) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
     if (n < 2 || (n & 1)) return PFB_ERR_SIZE;
     if (batch == 0) return PFB_OK;
     if (!A || !G_out || !log_out || !sign_out) return PFB_ERR_INVALID;
-    const size_t need = pfb::grad_workspace_bytes(dtype, batch, n, mode);
-    if (need == 0) return PFB_ERR_SIZE;
-    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
+    const size_t need1 = pfb::grad_workspace_bytes(dtype, 1, n, mode);   // one matrix at a time
+    if (need1 == 0) return PFB_ERR_SIZE;
+    if (!workspace || workspace_bytes < need1 || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
     const int rc = pfb::launch_grad(dtype, A, batch, n, layout, mode, ct_log, G_out, log_out, sign_out,
-                                    workspace, (cudaStream_t)stream);
+                                    workspace, workspace_bytes, (cudaStream_t)stream);
     if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
     return rc;
 }

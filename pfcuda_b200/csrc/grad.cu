@@ -22,10 +22,17 @@
 //   2. grad_fix_kernel: the interchanges of later panels are applied to the
 //      Gauss vectors of earlier panels (the forward pass skips this), and the
 //      permutation perm is built;
-//   3. grad_build_u_kernel: U as an explicit n x n matrix;
-//   4. grad_diag_inv_kernel: the 64 x 64 diagonal blocks of Y = U^-1, in parallel;
-//   5. grad_block_row_kernel, block rows from the bottom: Y_I,J>I = -Y_II (U_I,>I Y_>I,J);
-//   6. grad_scatter_kernel: Q Y^T on the upper tiles, scaled and scattered to G.
+//   3. grad_diag_inv_kernel: the 64 x 64 diagonal blocks of Y = U^-1, in parallel;
+//   4. grad_block_row_kernel, block rows from the bottom: Y_I,J>I = -Y_II (U_I,>I Y_>I,J);
+//   5. grad_scatter_kernel: Q Y^T on the upper tiles, scaled and scattered to G.
+// U is never stored: its entries are read from the Gauss vectors in W (u_entry).
+//
+// Memory budget: the workspace is the budget.  Per matrix the adjoint needs its
+// working matrix W (the factors) and Y, about 2 n^2 elements; a workspace that
+// holds fewer matrices than the batch makes the call run the batch in chunks of
+// as many matrices as fit, each chunk factored, differentiated and its storage
+// reused by the next.  Every matrix's arithmetic is independent of the others,
+// so the results do not depend on the chunking.
 #include "common.cuh"
 #include "large.cuh"
 #include "dmma.cuh"
@@ -35,7 +42,7 @@ namespace pfb {
 constexpr int kGB = 64;   // block size of the triangular inverse and of the output tiles
 
 struct GradLayout {
-    size_t large_bytes, u_off, y_off, perm_off, total;
+    size_t large_bytes, y_off, perm_off, total;
 };
 
 static size_t galign(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -45,8 +52,7 @@ static GradLayout grad_layout(int dtype, int64_t B, int n, int mode)
     GradLayout L{};
     const size_t ts = (dtype == PFB_C64 || dtype == PFB_C128) ? 16 : 8;
     L.large_bytes = galign(large_workspace_bytes(dtype, B, n, mode));
-    L.u_off = L.large_bytes;
-    L.y_off = galign(L.u_off + (size_t)B * n * n * ts);
+    L.y_off = L.large_bytes;
     L.perm_off = galign(L.y_off + (size_t)B * n * n * ts);
     L.total = galign(L.perm_off + (size_t)B * n * sizeof(int32_t));
     return L;
@@ -93,50 +99,38 @@ __global__ void grad_fix_kernel(T *__restrict__ W_all, const int32_t *__restrict
     }
 }
 
-// 3. U explicitly (full n x n: unit diagonal, zeros below and at (2t, 2t+1))
+// Entry (r, c) of U (unit diagonal, zeros below it and at (2t, 2t+1)) from the
+// Gauss vectors in W: row 2t+1 of U is u_t (row 2t of W), row 2t is w_t / a_t
+// (row 2t+1 of W over the pivot W[2t][2t+1]); ia = 1 / a_t of row r's pair.
 template <typename T>
-__global__ void grad_build_u_kernel(const T *__restrict__ W_all, T *__restrict__ U_all,
-                                    const MatState *__restrict__ st_all, int n)
+PFB_D T u_entry(const T *__restrict__ W, int n, int r, int c, T ia)
 {
-    const int64_t b = blockIdx.y;
-    if (st_all[b].dead) return;
-    const T *W = W_all + b * (int64_t)n * n;
-    T *U = U_all + b * (int64_t)n * n;
-    const int64_t nn = (int64_t)n * n;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(e / n), c = (int)(e % n);
-        T v = zero<T>();
-        if (c == r) {
-            v = one<T>();
-        } else if (c > (r | 1)) {
-            const int t = r >> 1;
-            if (r & 1) {
-                v = W[(int64_t)(2 * t) * n + c];
-            } else {
-                const T a = W[(int64_t)(2 * t) * n + 2 * t + 1];
-                v = W[(int64_t)(2 * t + 1) * n + c] * recip(a);
-            }
-        }
-        U[e] = v;
-    }
+    if (c == r) return one<T>();
+    if (c <= (r | 1)) return zero<T>();
+    const int t = r >> 1;
+    return (r & 1) ? W[(int64_t)(2 * t) * n + c] : W[(int64_t)(2 * t + 1) * n + c] * ia;
 }
 
-// 4. Y_II = U_II^-1 for every diagonal block (zeros outside the block's upper part).
+// 3. Y_II = U_II^-1 for every diagonal block (zeros outside the block's upper part).
 template <typename T>
 __global__ void __launch_bounds__(kGB)
-grad_diag_inv_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all, int n)
+grad_diag_inv_kernel(const T *__restrict__ W_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all, int n)
 {
     const int64_t b = blockIdx.y;
     if (st_all[b].dead) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Us = reinterpret_cast<T *>(smem_raw);          // [kGB][kGB]
     T *Ys = Us + kGB * kGB;
-    const T *U = U_all + b * (int64_t)n * n;
+    const T *W = W_all + b * (int64_t)n * n;
     T *Y = Y_all + b * (int64_t)n * n;
     const int r0 = blockIdx.x * kGB;
     const int sz = (n - r0) < kGB ? n - r0 : kGB;
     const int j = threadIdx.x;
-    for (int i = 0; i < kGB; i++) Us[i * kGB + j] = (i < sz && j < sz) ? U[(int64_t)(r0 + i) * n + r0 + j] : zero<T>();
+    for (int i = 0; i < kGB; i++) {
+        const int r = r0 + i;
+        const T ia = (i < sz && !(r & 1)) ? recip(W[(int64_t)r * n + r + 1]) : zero<T>();
+        Us[i * kGB + j] = (i < sz && j < sz) ? u_entry(W, n, r, r0 + j, ia) : zero<T>();
+    }
     __syncthreads();
     // column j of the inverse by back substitution, one thread per column
     for (int i = kGB - 1; i >= 0; i--) {
@@ -159,12 +153,12 @@ template <typename T> __host__ __device__ constexpr int ld_kc32() { return 36; }
 template <typename T> __host__ __device__ constexpr int ld_kc64() { return 68; }
 template <typename T> __host__ __device__ constexpr int ld_km64() { return IsComplex<T>::value ? 66 : 68; }
 
-// 5. one block row I of Y (rows r0 .. r0+63), column tile blockIdx.x after it:
+// 4. one block row I of Y (rows r0 .. r0+63), column tile blockIdx.x after it:
 // Y[I][c] = -Y_II * sum_{k >= r1} U[I][k] Y[k][c], both products on the FP64
 // tensor cores (8 warps, each a 32 x 16 block of m8n8k4 fragments).
 template <typename T>
 __global__ void __launch_bounds__(256)
-grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all,
+grad_block_row_kernel(const T *__restrict__ W_all, T *__restrict__ Y_all, const MatState *__restrict__ st_all,
                       int n, int r0)
 {
     const int64_t b = blockIdx.y;
@@ -175,8 +169,14 @@ grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const 
     T *Yt = Ut + kGB * LA;                           // [32][LB]   Y[k][c]   (k-major)
     T *Ts = reinterpret_cast<T *>(smem_raw);        // [kGB][LB]  the sum   (k-major), after the loop
     T *Yii = Ts + kGB * LB;                          // [kGB][LY]  Y_II      (k-contiguous)
-    const T *U = U_all + b * (int64_t)n * n;
+    __shared__ T ias[kGB / 2];                       // 1 / a_t of the block row's pairs
+    const T *W = W_all + b * (int64_t)n * n;
     T *Y = Y_all + b * (int64_t)n * n;
+    if (threadIdx.x < kGB / 2) {
+        const int r = r0 + 2 * threadIdx.x;
+        ias[threadIdx.x] = r + 1 < n ? recip(W[(int64_t)r * n + r + 1]) : zero<T>();
+    }
+    __syncthreads();
     const int r1 = r0 + kGB;
     const int c0 = r1 + blockIdx.x * kGB;
     const int tid = threadIdx.x, warp = tid >> 5, g = (tid & 31) >> 2, t = tid & 3;
@@ -187,7 +187,7 @@ grad_block_row_kernel(const T *__restrict__ U_all, T *__restrict__ Y_all, const 
     for (int k0 = r1; k0 < kend; k0 += 32) {
         for (int e = tid; e < kGB * 32; e += 256) {
             const int i = e / 32, k = e % 32;
-            Ut[i * LA + k] = (r0 + i < n && k0 + k < n) ? U[(int64_t)(r0 + i) * n + k0 + k] : zero<T>();
+            Ut[i * LA + k] = (r0 + i < n && k0 + k < n) ? u_entry(W, n, r0 + i, k0 + k, ias[i >> 1]) : zero<T>();
             const int kk = e / kGB, c = e % kGB;
             Yt[kk * LB + c] = (k0 + kk < n && c0 + c < n) ? Y[(int64_t)(k0 + kk) * n + c0 + c] : zero<T>();
         }
@@ -239,7 +239,7 @@ template <> PFB_D float to_out<double, float>(double v) { return (float)v; }
 template <> PFB_D c128 to_out<c128, c128>(c128 v) { return v; }
 template <> PFB_D c64 to_out<c128, c64>(c128 v) { return mk((float)v.re, (float)v.im); }
 
-// 6. M = Q Y^T on the upper 64 x 64 tiles, G[perm[r]][perm[c]] = -(ct/2) M[r][c]
+// 5. M = Q Y^T on the upper 64 x 64 tiles, G[perm[r]][perm[c]] = -(ct/2) M[r][c]
 // and its skew mirror, on the FP64 tensor cores.  Matrices with Pf = 0 get NaN.
 template <typename T, typename O>
 __global__ void __launch_bounds__(256)
@@ -342,22 +342,19 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
     if (rc != PFB_OK) return rc;
     const LargeView V = large_view(dtype, B, n, mode, ws);
     T *W = static_cast<T *>(V.W);
-    T *U = reinterpret_cast<T *>(ws + L.u_off);
     T *Y = reinterpret_cast<T *>(ws + L.y_off);
     int32_t *perm = reinterpret_cast<int32_t *>(ws + L.perm_off);
     const int nb = large_panel_width(dtype, n);
     const unsigned ub = (unsigned)B;
 
     grad_fix_kernel<T><<<dim3((n + 255) / 256, ub), 256, 0, s>>>(W, V.piv, perm, V.st, n, nb);
-    grad_build_u_kernel<T><<<dim3((unsigned)((int64_t)n * n / 256 + 1 < 1024 ? (int64_t)n * n / 256 + 1 : 1024), ub), 256, 0, s>>>(
-        W, U, V.st, n);
     const int nblk = (n + kGB - 1) / kGB;
     {
         auto k = grad_diag_inv_kernel<T>;
         const size_t sm = 2 * kGB * kGB * sizeof(T);
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
             return PFB_ERR_CUDA;
-        k<<<dim3((unsigned)nblk, ub), kGB, sm, s>>>(U, Y, V.st, n);
+        k<<<dim3((unsigned)nblk, ub), kGB, sm, s>>>(W, Y, V.st, n);
     }
     {
         auto k = grad_block_row_kernel<T>;
@@ -367,7 +364,7 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
         for (int I = nblk - 2; I >= 0; I--) {
             const int r0 = I * kGB;
             const int tiles = (n - (r0 + kGB) + kGB - 1) / kGB;
-            k<<<dim3((unsigned)tiles, ub), 256, sm, s>>>(U, Y, V.st, n, r0);
+            k<<<dim3((unsigned)tiles, ub), 256, sm, s>>>(W, Y, V.st, n, r0);
         }
     }
     {
@@ -394,13 +391,40 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
+// The largest number of matrices (<= batch) whose adjoint fits in `bytes` of
+// workspace; 0 if not even one does.
+int64_t grad_chunk(int dtype, int64_t batch, int n, int mode, size_t bytes)
+{
+    if (grad_workspace_bytes(dtype, 1, n, mode) > bytes) return 0;
+    int64_t lo = 1, hi = batch;
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo + 1) / 2;
+        if (grad_workspace_bytes(dtype, mid, n, mode) <= bytes) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 int launch_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode, const double *ct, void *G,
-                double *log_out, void *sign_out, void *workspace, cudaStream_t stream)
+                double *log_out, void *sign_out, void *workspace, size_t workspace_bytes, cudaStream_t stream)
 {
     unsigned char *ws = static_cast<unsigned char *>(workspace);
-    if (dtype == PFB_C64 || dtype == PFB_C128)
-        return run_grad<c128>(dtype, A, batch, n, layout, mode, ct, G, log_out, sign_out, ws, stream);
-    return run_grad<double>(dtype, A, batch, n, layout, mode, ct, G, log_out, sign_out, ws, stream);
+    const int64_t chunk = grad_chunk(dtype, batch, n, mode, workspace_bytes);
+    if (chunk <= 0) return PFB_ERR_WORKSPACE;
+    const size_t es = (dtype == PFB_F32) ? 4 : (dtype == PFB_C128 ? 16 : 8);
+    const size_t mat = (size_t)n * (size_t)n * es;
+    for (int64_t b0 = 0; b0 < batch; b0 += chunk) {
+        const int64_t B = batch - b0 < chunk ? batch - b0 : chunk;
+        const void *a = static_cast<const char *>(A) + (size_t)b0 * mat;
+        void *g = static_cast<char *>(G) + (size_t)b0 * mat;
+        void *so = static_cast<char *>(sign_out) + (size_t)b0 * es;
+        const double *c = ct ? ct + b0 : nullptr;
+        const int rc = (dtype == PFB_C64 || dtype == PFB_C128)
+                           ? run_grad<c128>(dtype, a, B, n, layout, mode, c, g, log_out + b0, so, ws, stream)
+                           : run_grad<double>(dtype, a, B, n, layout, mode, c, g, log_out + b0, so, ws, stream);
+        if (rc != PFB_OK) return rc;
+    }
+    return PFB_OK;
 }
 
 }  // namespace pfb

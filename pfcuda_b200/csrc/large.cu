@@ -417,7 +417,9 @@ static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_
         if (CL < 1) CL = 1;
         if (CL > kClusterMax) return PFB_ERR_SIZE;
         const bool use_split = (mode & 0xff) == PFB_MODE_SPLIT && mt > 0;
-        sa = split_shift(split_args(use_split, split_ws, cplx, batch, n, NB, k0, slices), b0);
+        sa = split_args(use_split, split_ws, cplx, batch, n, NB, k0, slices);
+        if (mode & PFB_SPLIT_TEST_TIMEOUT) sa.fail_b = 0;
+        sa = split_shift(sa, b0);
 
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)CL, (unsigned)B, 1);
@@ -525,16 +527,41 @@ static int run_large_range(int dtype, const void *A, int64_t batch, int64_t b0, 
     return run_large<c128, 32, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing);
 }
 
-// The second stream of a device's split calls (created once, never destroyed).
+// The second stream of this host thread's calls on device `dev`: one per thread
+// and device, created on first use and destroyed when the thread exits.  Per
+// thread, so that callers on other threads never share it: their calls stay
+// independent, and a graph capture on one thread cannot pull in another
+// thread's work.
+struct AuxStreams {
+    cudaStream_t s[64] = {};
+    ~AuxStreams()
+    {
+        for (cudaStream_t x : s)
+            if (x) cudaStreamDestroy(x);
+    }
+};
+
 static cudaStream_t aux_stream(int dev)
 {
-    static std::mutex mu;
-    static cudaStream_t streams[64] = {};
-    std::lock_guard<std::mutex> lock(mu);
+    thread_local AuxStreams aux;
     if (dev < 0 || dev >= 64) return nullptr;
-    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
-        streams[dev] = nullptr;
-    return streams[dev];
+    if (!aux.s[dev] && cudaStreamCreateWithFlags(&aux.s[dev], cudaStreamNonBlocking) != cudaSuccess)
+        aux.s[dev] = nullptr;
+    return aux.s[dev];
+}
+
+// Whether work forked from `caller` onto `aux` stays in the caller's own
+// capture state: a stream that joined a graph capture belongs to it until that
+// capture ends, so while `aux` is part of a capture, only a call on a stream of
+// that same capture may use it.
+static bool aux_usable(cudaStream_t caller, cudaStream_t aux)
+{
+    cudaStreamCaptureStatus ca = cudaStreamCaptureStatusNone, cc = cudaStreamCaptureStatusNone;
+    unsigned long long ia = 0, ic = 0;
+    if (cudaStreamGetCaptureInfo(aux, &ca, &ia) != cudaSuccess) return false;
+    if (ca == cudaStreamCaptureStatusNone) return true;
+    if (cudaStreamGetCaptureInfo(caller, &cc, &ic) != cudaSuccess) return false;
+    return ca == cudaStreamCaptureStatusActive && cc == cudaStreamCaptureStatusActive && ia == ic;
 }
 
 // A batch of three or more waves of the widest panel clusters (clusters of 9
@@ -543,7 +570,20 @@ static cudaStream_t aux_stream(int dev)
 // updates fill the SMs the first range's panel waves leave idle (2n = 4096,
 // batch 28: 43.0 -> 41.9 ms).  The second stream forks from and joins the
 // caller's stream through events, so the call stays ordered on `stream` and
-// can be captured in a CUDA graph.
+// can be captured in a CUDA graph.  The second stream is this host thread's own
+// (aux_stream); when it is part of another capture the call runs as one range.
+//
+// The size of the second range (0: one range) for a call on `batch` matrices.
+int64_t large_second_range(int dtype, int64_t batch, int n)
+{
+    int nb = 0, cpt = 0;
+    if (!large_cfg(dtype, n, &nb, &cpt)) return 0;
+    const int widest = (n - nb + kTT * cpt - 1) / (kTT * cpt);
+    if (widest < 9) return 0;
+    const int mc = large_max_concurrent(dtype, n);
+    return (mc > 0 && batch >= 3 * (int64_t)mc) ? mc : 0;
+}
+
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
                  cudaStream_t stream, const pfb_slog_timing *timing)
@@ -553,11 +593,11 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
     if ((mode & 0xff) == PFB_MODE_SPLIT && !split_available()) return PFB_ERR_UNSUPPORTED;
     if (batch > 65535) return PFB_ERR_SIZE;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
-    const int widest = (n - nb + kTT * cpt - 1) / (kTT * cpt);
-    const int mc = (timing == nullptr && widest >= 9) ? large_max_concurrent(dtype, n) : 0;
+    const int64_t mc = timing == nullptr ? large_second_range(dtype, batch, n) : 0;
     int dev = 0;
     cudaStream_t s2 = nullptr;
-    if (mc > 0 && batch >= 3 * (int64_t)mc && cudaGetDevice(&dev) == cudaSuccess) s2 = aux_stream(dev);
+    if (mc > 0 && cudaGetDevice(&dev) == cudaSuccess) s2 = aux_stream(dev);
+    if (s2 && !aux_usable(stream, s2)) s2 = nullptr;
     if (!s2) return run_large_range(dtype, A, batch, 0, batch, n, layout, mode, log_out, sign_out, ws, stream, timing);
 
     const int64_t B2 = mc, B1 = batch - B2;

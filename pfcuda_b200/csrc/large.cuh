@@ -26,6 +26,7 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
 
 int large_panel_width(int dtype, int n);
 int large_max_concurrent(int dtype, int n);
+int64_t large_second_range(int dtype, int64_t batch, int n);
 
 // Where the factorisation leaves its results inside a large-path workspace:
 // the pivot columns (n/2 per matrix), the per-matrix state, and W, the
@@ -40,8 +41,9 @@ LargeView large_view(int dtype, int64_t batch, int n, int mode, void *workspace)
 
 // Declared here, defined in grad.cu: the adjoint of log|Pf|.
 size_t grad_workspace_bytes(int dtype, int64_t batch, int n, int mode);
+int64_t grad_chunk(int dtype, int64_t batch, int n, int mode, size_t bytes);
 int launch_grad(int dtype, const void *A, int64_t batch, int n, int layout, int mode, const double *ct, void *G,
-                double *log_out, void *sign_out, void *workspace, cudaStream_t stream);
+                double *log_out, void *sign_out, void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 size_t ragged_workspace_bytes(int64_t count, int max_n);
 int launch_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, int64_t count, int max_n,

@@ -11,17 +11,18 @@
 // array until the process exits.
 //
 // In host code the array's name is only a host-side stand-in, never a device
-// address, so its device address is looked up once per device (with that
-// device current) by cudaGetSymbolAddress on the first call made on the device,
-// and that address is what the kernels are given.
+// address, so every call looks up its device address on the current device
+// with cudaGetSymbolAddress (a cheap query once the module is loaded) and
+// hands that address to the kernels.  Nothing is cached, so a device reset or
+// a new context between calls cannot leave a stale address behind.  The first
+// call on a device loads the library's module there, so make that first call
+// before any stream capture.
 //
 // All calls share the array, and it keeps the last call's contents.  Nothing of
 // it has to start at zero: the factorisation's first kernel overwrites the
 // working matrix and the per-matrix state it later reads, and every pivot is
 // written before it is read.  Calls whose work overlaps on the GPU (two streams,
 // or two host threads) race on the array and must be serialised by the caller.
-#include <mutex>
-
 #include "common.cuh"
 #include "small.cuh"
 #include "large.cuh"
@@ -30,23 +31,12 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PFB_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-void *g_scratch_addr[kMaxDevices];
-
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// Device address of g_noalloc_scratch on the current device.
 int scratch_address(void **out)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return PFB_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return PFB_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PFB_ERR_CUDA;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PFB_ERR_CUDA;
+    *out = p;
     return PFB_OK;
 }
 

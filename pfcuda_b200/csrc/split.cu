@@ -83,6 +83,7 @@ SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int 
     int8_t *end = (cplx ? a.ys2 : a.ys) + batch * a.mstride;
     a.ex = reinterpret_cast<int32_t *>(end);
     a.err = a.ex + batch * (int64_t)n;
+    a.fail_b = -1;
     return a;
 }
 
@@ -107,9 +108,9 @@ PFB_D bool mbar_try_wait(uint32_t bar, uint32_t parity)
                  : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
     return ok != 0;
 }
-PFB_D bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
+PFB_D bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit = kWaitSpins)
 {
-    for (long long i = 0; i < kWaitSpins; i++)
+    for (long long i = 0; i < limit; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -332,6 +333,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     const int ntiles = t1 - t0;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // the polls of every wait of the pipeline (the drain after a failure below
+    // keeps the full bound): none for the matrix PFB_SPLIT_TEST_TIMEOUT marks
+    const long long lim = ((int)b == sa.fail_b) ? 0 : kWaitSpins;
     // mbarrier i sits at bar0 + 8 i (an address, not an array: a runtime index
     // into a register array would move it to local memory)
     const uint32_t bar0 = su32(bars);
@@ -364,7 +368,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             int arow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, tw.step()) {
                 if (tw.I != arow) {
-                    if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1);
+                    if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1, lim);
                     if (!ok) break;
                     mbar_expect_tx(mb(0), (uint32_t)(S * a_bytes));
                     for (int s = 0; s < S; s++)
@@ -374,7 +378,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
                     aloads++;
                     p_aloads = aloads;
                 }
-                if (it >= 1) ok = mbar_wait_bounded(mb(3), (it - 1) & 1);
+                if (it >= 1) ok = mbar_wait_bounded(mb(3), (it - 1) & 1, lim);
                 if (!ok) break;
                 const int jrow = tw.J * TN;
                 const int64_t boff = (int64_t)(jrow / TM) * chunk + (int64_t)((jrow % TM) >> 3) * (kk >> 4) * 128;
@@ -404,13 +408,13 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             for (int it = 0; it < ntiles && ok; it++, tw.step()) {
                 if (tw.I != arow) {
                     if (aloads > 0) mma_commit(mb(1));          // A may be replaced once these MMAs finish
-                    ok = mbar_wait_bounded(mb(0), aloads & 1);
+                    ok = mbar_wait_bounded(mb(0), aloads & 1, lim);
                     if (!ok) break;
                     arow = tw.I;
                     aloads++;
                 }
-                ok = mbar_wait_bounded(mb(2), it & 1);
-                if (ok && it >= 1) ok = mbar_wait_bounded(mb(5), (it - 1) & 1);
+                ok = mbar_wait_bounded(mb(2), it & 1, lim);
+                if (ok && it >= 1) ok = mbar_wait_bounded(mb(5), (it - 1) & 1, lim);
                 if (!ok) break;
                 tc_fence_after();
 #pragma unroll
@@ -469,9 +473,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             const int bc0 = k1 + tw.J * TN + h * CW;
             const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
             const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
-            bool w_ok = mbar_wait_bounded(mb(6 + buf), (it >> 1) & 1);
+            bool w_ok = mbar_wait_bounded(mb(6 + buf), (it >> 1) & 1, lim);
             if (w_ok) c_done = it + 1;
-            if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1);
+            if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1, lim);
             ok = epi_all(w_ok);
             if (!ok) break;
             tc_fence_after();

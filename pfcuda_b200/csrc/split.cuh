@@ -35,6 +35,8 @@ struct SplitArgs {
     int8_t *ys2;              // complex only: [Yi | Yr]
     int32_t *ex;              // [B][n] power-of-two exponent per trailing index
     int32_t *err;             // [B] device-side timeout flags of the update kernel
+    int fail_b;               // matrix (of this range) whose waits give up at once, -1: none
+                              // (PFB_SPLIT_TEST_TIMEOUT, which exercises the timeout path)
 };
 
 size_t split_workspace_bytes(bool cplx, int64_t batch, int n, int nb);
@@ -48,6 +50,7 @@ inline SplitArgs split_shift(SplitArgs a, int64_t b0)
     if (a.ys2) a.ys2 += b0 * a.mstride;
     a.ex += b0 * (int64_t)a.n;
     a.err += b0;
+    a.fail_b = (a.fail_b >= 0 && a.fail_b >= b0) ? (int)(a.fail_b - b0) : -1;
     return a;
 }
 bool split_available();

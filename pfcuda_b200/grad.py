@@ -24,9 +24,14 @@ def grad_workspace_bytes(dtype: torch.dtype, batch: int, n: int, mode: str = "fp
     return int(_lib.lib().pfb_slog_grad_workspace_bytes(_DT[dtype], batch, n, _MODES[mode]))
 
 
+def grad_min_workspace_bytes(dtype: torch.dtype, n: int, mode: str = "fp64") -> int:
+    """The smallest workspace the adjoint accepts: one matrix at a time."""
+    return grad_workspace_bytes(dtype, 1, n, mode)
+
+
 def slog_pfaffian_grad(A: torch.Tensor, ct: torch.Tensor | None = None, mode: str = "fp64",
                        layout: int = _lib.ROW_MAJOR, workspace: torch.Tensor | None = None,
-                       return_forward: bool = False):
+                       return_forward: bool = False, budget_bytes: int | None = None):
     """ct * d log Pf(A) / dA = ct * (1/2) A^-T for a contiguous (..., n, n) CUDA tensor.
 
     ``ct`` holds one real cotangent per matrix (None: all ones).  The result has
@@ -34,6 +39,12 @@ def slog_pfaffian_grad(A: torch.Tensor, ct: torch.Tensor | None = None, mode: st
     Pf = 0 gets an all-NaN gradient; odd orders (Pf = 0 identically) give NaN
     without a launch.  With ``return_forward`` the call also returns
     (log|Pf|, sign) of the same factorisation.
+
+    ``budget_bytes`` caps the workspace (about 2 n^2 working elements per
+    matrix): the batch then runs in chunks of as many matrices as fit, with
+    results identical to an unbounded call.  It cannot go below one matrix's
+    need (grad_min_workspace_bytes).  A ``workspace`` tensor given by the caller
+    is used as it is, its size being the budget.
     """
     if not isinstance(A, torch.Tensor) or not A.is_cuda:
         raise ValueError("the engine runs on CUDA tensors only (no CPU fallback)")
@@ -60,8 +71,17 @@ def slog_pfaffian_grad(A: torch.Tensor, ct: torch.Tensor | None = None, mode: st
     wsb = grad_workspace_bytes(A.dtype, B, n, mode)
     if wsb == 0:
         raise ValueError(f"order {n} is outside the supported range")
-    if workspace is None or workspace.numel() < wsb:
+    w1 = grad_min_workspace_bytes(A.dtype, n, mode)
+    if budget_bytes is not None:
+        if budget_bytes < w1:
+            raise ValueError(f"budget_bytes {budget_bytes} is below one matrix's need ({w1} bytes)")
+        wsb = min(wsb, int(budget_bytes))
+    if workspace is None:
         workspace = torch.empty(wsb, dtype=torch.uint8, device=A.device)
+    elif workspace.numel() < w1:
+        raise ValueError(f"workspace of {workspace.numel()} bytes is below one matrix's need ({w1} bytes)")
+    else:
+        wsb = min(wsb, workspace.numel())
     st = _lib.lib().pfb_slog_pfaffian_grad(
         _DT[A.dtype], A.data_ptr(), B, n, layout, _MODES[mode],
         ct.data_ptr() if ct is not None else None, G.data_ptr(), la.data_ptr(), sg.data_ptr(),

@@ -184,3 +184,96 @@ def test_grad_ignores_lower_triangle():
         G1, l1, s1 = run(A)
         G2, l2, s2 = run(D)
         assert np.array_equal(G1, G2) and np.array_equal(l1, l2) and np.array_equal(s1, s2)
+
+
+# ------------------------------------------------------------ forward mode
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_forward_mode_slog(cplx):
+    """torch.func.jvp of slog_pfaffian through the engine: the tangent of
+    log|Pf| is Re (1/2) tr(A^-1 dA) (the reference's rule, pfcuda/cuda_api.py:
+    92-107, restated with NumPy's inverse), and matches central differences
+    along skew directions; the phase of complex A turns by i Im of the trace."""
+    rng = np.random.default_rng(300 + cplx)
+    n = 130
+    A = O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n), complex_=cplx)
+    E = O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n), complex_=cplx)
+    (la, sg), (dla, dsg) = torch.func.jvp(lambda X: pf.slog_pfaffian(X, mode="fp64"), (cuda(A),), (cuda(E),))
+    t = O.slog_pf_jvp(A, E)
+    assert np.all(np.abs(dla.cpu().numpy() - np.real(t)) <= 1e-9 * np.abs(t) + 1e-10)
+    assert np.all(np.abs(dla.cpu().numpy() - O.fd_slog(A, E)) <= 1e-6 * np.abs(t) + 1e-8)
+    if cplx:
+        want = sg.cpu().numpy() * 1j * np.imag(t)
+        assert np.all(np.abs(dsg.cpu().numpy() - want) <= 1e-9 * np.abs(t) + 1e-10)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_forward_mode_pfaffian(cplx):
+    """torch.func.jvp of pfaffian: d Pf = Pf (1/2) tr(A^-1 dA) (pfcuda/cuda_api.py:78-90)."""
+    rng = np.random.default_rng(310 + cplx)
+    A = O.skew_normal(rng, 16, 24, complex_=cplx)
+    E = O.skew_normal(rng, 16, 24, complex_=cplx)
+    p, dp = torch.func.jvp(pf.pfaffian, (cuda(A),), (cuda(E),))
+    want = O.pf_product(A) * O.slog_pf_jvp(A, E)
+    assert np.all(np.abs(dp.cpu().numpy() - want) <= 1e-9 * np.abs(want) + 1e-9)
+
+
+# ------------------------------------------------------------ memory budget
+
+@pytest.mark.parametrize("mode", ["fp64", "split"])
+def test_budget_chunks_are_bit_identical(mode):
+    """A workspace below the whole batch's need runs the batch in chunks of as
+    many matrices as fit; the gradients and forward values equal those of one
+    unbounded call bit for bit, down to one matrix at a time."""
+    from pfcuda_b200.grad import grad_min_workspace_bytes, grad_workspace_bytes
+    rng = np.random.default_rng(320)
+    n, B = 160, 7
+    A = cuda(O.skew_normal(rng, B, n, scale=1 / np.sqrt(n)))
+    ct = cuda(np.linspace(-1.0, 2.0, B))
+    full = pf.slog_pfaffian_grad(A, ct=ct, mode=mode, return_forward=True)
+    w1 = grad_min_workspace_bytes(A.dtype, n, mode)
+    assert w1 < grad_workspace_bytes(A.dtype, B, n, mode)
+    for budget in (w1, 3 * w1 - 1, grad_workspace_bytes(A.dtype, 3, n, mode)):
+        got = pf.slog_pfaffian_grad(A, ct=ct, mode=mode, return_forward=True, budget_bytes=budget)
+        for x, y in zip(got, full):
+            assert torch.equal(x, y)
+    with pytest.raises(ValueError):
+        pf.slog_pfaffian_grad(A, budget_bytes=w1 - 1)
+
+
+def test_budget_below_one_matrix_is_refused_by_the_c_abi():
+    from pfcuda_b200.grad import grad_min_workspace_bytes
+    n = 66
+    A = cuda(np.zeros((2, n, n)))
+    w1 = grad_min_workspace_bytes(A.dtype, n, "fp64")
+    ws = torch.empty(w1, dtype=torch.uint8, device="cuda")
+    G = torch.empty_like(A)
+    la = torch.empty(2, dtype=torch.float64, device="cuda")
+    sg = torch.empty(2, dtype=torch.float64, device="cuda")
+    L = _lib.lib()
+    s = torch.cuda.current_stream().cuda_stream
+    st = L.pfb_slog_pfaffian_grad(_lib.F64, A.data_ptr(), 2, n, 0, 0, None, G.data_ptr(), la.data_ptr(),
+                                  sg.data_ptr(), ws.data_ptr(), w1 - 256, s)
+    assert st == 3                                  # PFB_ERR_WORKSPACE
+    st = L.pfb_slog_pfaffian_grad(_lib.F64, A.data_ptr(), 2, n, 0, 0, None, G.data_ptr(), la.data_ptr(),
+                                  sg.data_ptr(), ws.data_ptr(), w1, s)
+    assert st == 0
+
+
+# ------------------------------------------------- ill-conditioned, exact
+
+@pytest.mark.parametrize("mode", ["fp64", "split"])
+def test_grad_ill_conditioned_vs_exact_inverse(mode):
+    """The ill-conditioned construction A = Q blockdiag(s_k J) Q^T (s_k in
+    [1e-6, 1], cond_2 = 1e6) has the exact adjoint (1/2) Q blockdiag(J/s_k) Q^T,
+    formed from the stored Q (oracle.illcond_half_inv_t).  Bar: relative
+    Frobenius error <= cond_2 * sqrt(n) * eps * 4 (about 2e-8 at 2n = 2048),
+    well below the worst-case cond * n * eps = 2.3e-7 that a general inverse may
+    reach; the forward error of the input's own rounding (about cond * eps)
+    sits below it."""
+    A, logs, signs, Q = O.config_illcond(B=2, n=2048, return_q=True)
+    G = pf.slog_pfaffian_grad(cuda(A), mode=mode).cpu().numpy()
+    Gx = O.illcond_half_inv_t(Q)
+    err = rel(G, Gx)
+    bar = 1e6 * np.sqrt(2048) * np.finfo(np.float64).eps * 4
+    assert np.all(err <= bar), (err, bar)

@@ -212,6 +212,9 @@ def test_two_stream_batches_match_single_ranges(mode):
     mc = _lib.lib().pfb_slog_max_concurrent(_lib.F64, n)
     assert mc > 0
     B = 3 * mc
+    # the call under test does run as two ranges, and a one-wave call as one
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n) == 2
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, mc, n) == 1
     rng = np.random.default_rng(77)
     A = O.skew_normal(rng, B, n, scale=1 / np.sqrt(n))
     At = cuda(A)
@@ -223,3 +226,92 @@ def test_two_stream_batches_match_single_ranges(mode):
     wl, ws = O.slog_pf(A[-2:])
     got = la[-2:].cpu().numpy()
     assert np.all(np.abs(got - wl) <= 1e-10 * np.abs(wl)) and np.array_equal(sg[-2:].cpu().numpy(), ws)
+
+
+def _two_range_batch(seed):
+    n = 2176
+    mc = _lib.lib().pfb_slog_max_concurrent(_lib.F64, n)
+    B = 3 * mc
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n) == 2
+    rng = np.random.default_rng(seed)
+    return cuda(O.skew_normal(rng, B, n, scale=1 / np.sqrt(n)))
+
+
+def test_two_threads_call_at_once():
+    """Two host threads, each on its own stream, run two-range calls at the same
+    time; each thread's second stream is its own, so every result equals the
+    one of the same call made alone, bit for bit."""
+    import threading
+    ins = [_two_range_batch(90 + i) for i in range(2)]
+    alone = [pf.slog_pfaffian_raw(X, mode="split") for X in ins]
+    torch.cuda.synchronize()
+    out = [None, None]
+    errs = []
+
+    def work(i):
+        try:
+            s = torch.cuda.Stream()
+            with torch.cuda.stream(s):
+                res = [pf.slog_pfaffian_raw(ins[i], mode="split") for _ in range(3)]
+            s.synchronize()
+            out[i] = res
+        except Exception as e:          # surfaced on the main thread below
+            errs.append(e)
+
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errs, errs
+    for i in range(2):
+        for la, sg in out[i]:
+            assert torch.equal(la, alone[i][0]) and torch.equal(sg, alone[i][1])
+
+
+def test_graph_capture_of_two_ranges():
+    """A two-range call captured in a CUDA graph (the second stream forks from
+    and joins the capturing stream) replays to the uncaptured results."""
+    X = _two_range_batch(95)
+    n, B = X.shape[-1], X.shape[0]
+    wsb = pf.slog_workspace_bytes(X.dtype, B, n, "split")
+    ws = torch.empty(wsb, dtype=torch.uint8, device=X.device)
+    want = pf.slog_pfaffian_raw(X, mode="split", workspace=ws)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        la, sg = pf.slog_pfaffian_raw(X, mode="split", workspace=ws)
+    for _ in range(2):
+        la.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(la, want[0]) and torch.equal(sg, want[1])
+
+
+def test_split_timeout_path_marks_only_its_matrix():
+    """PFB_SPLIT_TEST_TIMEOUT makes every bounded wait of the split update give
+    up at once for the call's first matrix: that matrix comes back as
+    (NaN, 0), the others are exact, and the device stays usable (a normal call
+    right after is exact for all)."""
+    rng = np.random.default_rng(41)
+    n, B = 256, 3
+    A = O.skew_normal(rng, B, n, scale=1 / np.sqrt(n))
+    X = cuda(A)
+    L = _lib.lib()
+    wsb = pf.slog_workspace_bytes(X.dtype, B, n, "split")
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    la = torch.empty(B, dtype=torch.float64, device="cuda")
+    sg = torch.empty(B, dtype=torch.float64, device="cuda")
+    mode = _lib.MODE_SPLIT | (1 << 12)           # PFB_SPLIT_TEST_TIMEOUT
+    st = L.pfb_slog_pfaffian(_lib.F64, X.data_ptr(), B, n, _lib.ROW_MAJOR, mode, la.data_ptr(), sg.data_ptr(),
+                             ws.data_ptr(), wsb, torch.cuda.current_stream().cuda_stream)
+    assert st == 0
+    torch.cuda.synchronize()
+    got_l, got_s = la.cpu().numpy(), sg.cpu().numpy()
+    wl, wsg = O.slog_pf(A)
+    assert np.isnan(got_l[0]) and got_s[0] == 0
+    assert np.all(np.abs(got_l[1:] - wl[1:]) <= 1e-10 * np.abs(wl[1:]))
+    assert np.array_equal(got_s[1:], wsg[1:])
+    la2, sg2 = pf.slog_pfaffian_raw(X, mode="split")
+    assert np.all(np.abs(la2.cpu().numpy() - wl) <= 1e-10 * np.abs(wl))
+    assert np.array_equal(sg2.cpu().numpy(), wsg)
