@@ -134,6 +134,48 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
                             void *workspace, size_t workspace_bytes, void *stream,
                             const pfb_slog_timing *timing);
 
+/*
+ * Settings of the large path that do not change its results' meaning, only
+ * how the work maps onto the GPU (and, for the split update, how many int8
+ * digits carry each operand).  Zero fields take the tuned table's choice for
+ * (dtype, n, batch): a table measured on the B200 by pfcuda_b200/tune.py and
+ * compiled into the library (pfcuda_b200/tune_table.json).
+ *   panel:  PFB_PANEL_REGISTERS -- each trailing column's panel rows in the
+ *           registers of one thread, one CTA per SM;
+ *           PFB_PANEL_HALF_SHARED -- half of those rows in shared memory, two
+ *           CTAs per SM, twice as many matrices' panels at once (orders whose
+ *           panel puts one trailing column per thread: up to 4160 real,
+ *           2080 complex).
+ *           Both forms choose the same pivots and round identically.
+ *   slices: int8 digits per operand of the split update (1..7); the mode's
+ *           PFB_SPLIT_DIGITS bits, when set, take precedence over the table.
+ *   ranges: 1 -- one stream; 2 -- a batch of three or more waves of the widest
+ *           panel clusters runs as two ranges (pfb_slog_stream_ranges).
+ */
+typedef enum {
+    PFB_PANEL_REGISTERS = 1,
+    PFB_PANEL_HALF_SHARED = 2
+} pfb_panel_form;
+
+typedef struct {
+    int panel;
+    int slices;
+    int ranges;
+} pfb_slog_config;
+
+/* The configuration a pfb_slog_pfaffian call on these arguments uses (the
+ * tuned table's choice), in *out.  Returns PFB_ERR_SIZE for orders outside the
+ * large path. */
+int pfb_slog_config_for(int dtype, int64_t batch, int n, int mode, pfb_slog_config *out);
+
+/* pfb_slog_pfaffian_timed with the configuration's non-zero fields in place of
+ * the table's (config may be NULL); PFB_ERR_INVALID for a field out of range or
+ * a panel form the order does not have. */
+int pfb_slog_pfaffian_ex(int dtype, const void *A, int64_t batch, int n, int layout,
+                         int mode, double *log_out, void *sign_out,
+                         void *workspace, size_t workspace_bytes, void *stream,
+                         const pfb_slog_timing *timing, const pfb_slog_config *config);
+
 /* Panel width (pivot rows per panel) the blocked factorisation uses for this
  * dtype and order; 0 if the order is not supported. */
 int pfb_slog_panel_width(int dtype, int n);
@@ -142,16 +184,23 @@ int pfb_slog_panel_width(int dtype, int n);
  * How many matrices of order n the current device factors concurrently: the
  * number of panel thread-block clusters (one per matrix, up to 16 CTAs) that
  * can be resident at once for the widest panel of the factorisation, as the
- * CUDA occupancy calculator reports it (7 on a B200 for 2n = 4096).  A batch of
- * this many matrices keeps every panel in one wave.  Returns 0 for orders the
- * large path does not take, or without a device.  No reference counterpart.
+ * CUDA occupancy calculator reports it, for the PFB_PANEL_REGISTERS form (7 on
+ * a B200 for 2n = 4096; PFB_PANEL_HALF_SHARED fits about twice as many).  A
+ * batch of this many matrices keeps every panel in one wave.  Returns 0 for
+ * orders the large path does not take, or without a device.  No reference
+ * counterpart.
  */
 int pfb_slog_max_concurrent(int dtype, int n);
 
+/* The same count for a given panel form (pfb_panel_form); 0 if the order does
+ * not have that form. */
+int pfb_slog_max_concurrent_form(int dtype, int n, int panel);
+
 /*
  * How many ranges a pfb_slog_pfaffian call on `batch` matrices of order n runs
- * as (1 or 2).  A batch of three or more waves of the widest panel clusters
- * (clusters of 9 or more CTAs) is split in two: the last wave's worth of
+ * as (1 or 2), for the tuned table's configuration in `mode` (PFB_MODE_*).  When
+ * the configuration asks for two ranges, a batch of three or more waves of the
+ * widest panel clusters (clusters of 9 or more CTAs) is split in two: the last wave's worth of
  * matrices runs on a second stream that forks from and joins `stream` through
  * events, so its trailing updates fill the SMs the first range's panel waves
  * leave idle.  The second stream belongs to the calling host thread (one per
@@ -160,7 +209,7 @@ int pfb_slog_max_concurrent(int dtype, int n);
  * thread's second stream is part of another graph capture runs as one range.
  * Each range launches its own sequence of kernels.  No reference counterpart.
  */
-int pfb_slog_stream_ranges(int dtype, int64_t batch, int n);
+int pfb_slog_stream_ranges(int dtype, int64_t batch, int n, int mode);
 
 /*
  * (log|Pf|, sign) of a ragged batch in one launch: `count` matrices of even (or

@@ -7,9 +7,10 @@ of include/pfb200.h (libpfb200.so, built in-tree).
 """
 from .api import (pfaffian, slog_pfaffian, pfaffian_raw, slog_pfaffian_raw,
                   slog_workspace_bytes, slog_pfaffian_ragged, RaggedPlan, upload_upper,
-                  upload_upper_bytes, resolve_mode)
+                  upload_upper_bytes, resolve_mode, slog_config)
 from .grad import slog_pfaffian_grad, grad_workspace_bytes
 
 __all__ = ["pfaffian", "slog_pfaffian", "pfaffian_raw", "slog_pfaffian_raw",
            "slog_workspace_bytes", "slog_pfaffian_ragged", "RaggedPlan",
-           "slog_pfaffian_grad", "grad_workspace_bytes", "upload_upper", "upload_upper_bytes", "resolve_mode"]
+           "slog_pfaffian_grad", "grad_workspace_bytes", "upload_upper", "upload_upper_bytes", "resolve_mode",
+           "slog_config"]

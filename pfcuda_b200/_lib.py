@@ -32,7 +32,10 @@ SIGNATURES = {
     "pfb_slog_pfaffian_timed": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _sz, _vp, _vp]),
     "pfb_slog_panel_width": (_int, [_int, _int]),
     "pfb_slog_max_concurrent": (_int, [_int, _int]),
-    "pfb_slog_stream_ranges": (_int, [_int, _i64, _int]),
+    "pfb_slog_stream_ranges": (_int, [_int, _i64, _int, _int]),
+    "pfb_slog_max_concurrent_form": (_int, [_int, _int, _int]),
+    "pfb_slog_config_for": (_int, [_int, _i64, _int, _int, _vp]),
+    "pfb_slog_pfaffian_ex": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),
     "pfb_slog_pfaffian_ragged": (_int, [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp, _sz, _vp]),
     "pfb_slog_ragged_workspace_bytes": (_sz, [_i64, _int]),
     "pfb_slog_pfaffian_noalloc": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp]),
@@ -41,6 +44,18 @@ SIGNATURES = {
     "pfb_upload_upper": (_int, [_int, _vp, _vp, _i64, _int, _vp]),
     "pfb_upload_upper_bytes": (_sz, [_int, _i64, _int]),
 }
+
+class SlogConfig(ctypes.Structure):
+    """pfb_slog_config of include/pfb200.h (0 fields: the tuned table's choice)."""
+    _fields_ = [("panel", ctypes.c_int), ("slices", ctypes.c_int), ("ranges", ctypes.c_int)]
+
+    def as_dict(self):
+        return {"panel": {1: "registers", 2: "half_shared"}.get(self.panel, self.panel),
+                "slices": self.slices, "ranges": self.ranges}
+
+
+PANEL_REGISTERS, PANEL_HALF_SHARED = 1, 2
+
 
 class SlogTiming(ctypes.Structure):
     """pfb_slog_timing of include/pfb200.h."""

@@ -15,6 +15,8 @@ adjoint kernel (pfcuda_b200.grad).
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -137,9 +139,31 @@ def slog_workspace_bytes(dtype: torch.dtype, batch: int, n: int, mode: str = "sp
     return int(_lib.lib().pfb_slog_workspace_bytes(_DT[dtype], batch, n, _MODES[mode]))
 
 
+def _config(config):
+    """A pfb_slog_config from a dict (panel: "registers" | "half_shared" | 1 | 2,
+    slices: 1..7, ranges: 1 | 2; missing keys take the tuned table's choice)."""
+    if config is None:
+        return None
+    panel = config.get("panel", 0)
+    panel = {"registers": _lib.PANEL_REGISTERS, "half_shared": _lib.PANEL_HALF_SHARED}.get(panel, panel)
+    return _lib.SlogConfig(int(panel), int(config.get("slices", 0)), int(config.get("ranges", 0)))
+
+
+def slog_config(dtype: torch.dtype, batch: int, n: int, mode: str = "split") -> dict:
+    """The configuration (panel form, split digits, stream ranges) that the
+    tuned table picks for a pfb_slog_pfaffian call on these arguments."""
+    c = _lib.SlogConfig()
+    _lib.check(_lib.lib().pfb_slog_config_for(_DT[dtype], batch, n, _MODES[mode], ctypes.byref(c)),
+               "pfb_slog_config_for")
+    return c.as_dict()
+
+
 def slog_pfaffian_raw(A: torch.Tensor, mode: str = "split", layout: int = _lib.ROW_MAJOR,
-                      workspace: torch.Tensor | None = None, return_pivots: bool = False):
-    """One pfb_slog_pfaffian call on a contiguous (..., n, n) CUDA tensor, any even n."""
+                      workspace: torch.Tensor | None = None, return_pivots: bool = False,
+                      config: dict | None = None):
+    """One pfb_slog_pfaffian call on a contiguous (..., n, n) CUDA tensor, any even n.
+
+    ``config`` overrides the tuned table's settings (see ``slog_config``)."""
     n = A.shape[-1]
     lead = A.shape[:-2]
     B = int(np.prod(lead)) if len(lead) else 1
@@ -148,9 +172,10 @@ def slog_pfaffian_raw(A: torch.Tensor, mode: str = "split", layout: int = _lib.R
     wsb = slog_workspace_bytes(A.dtype, B, n, mode)
     if workspace is None or workspace.numel() < wsb:
         workspace = torch.empty(max(wsb, 1), dtype=torch.uint8, device=A.device)
-    st = _lib.lib().pfb_slog_pfaffian(_DT[A.dtype], A.data_ptr(), B, n, layout, _MODES[mode],
-                                      la.data_ptr(), sg.data_ptr(), workspace.data_ptr(), wsb,
-                                      _stream(A))
+    cfg = _config(config)
+    st = _lib.lib().pfb_slog_pfaffian_ex(_DT[A.dtype], A.data_ptr(), B, n, layout, _MODES[mode],
+                                         la.data_ptr(), sg.data_ptr(), workspace.data_ptr(), wsb,
+                                         _stream(A), None, ctypes.byref(cfg) if cfg is not None else None)
     _lib.check(st, "pfb_slog_pfaffian")
     if return_pivots:
         piv = torch.empty(lead + (n // 2,), dtype=torch.int32, device=A.device)

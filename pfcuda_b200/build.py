@@ -28,8 +28,67 @@ def _nvcc():
     return cand if os.path.exists(cand) else "nvcc"
 
 
+TUNE_JSON = os.path.join(HERE, "tune_table.json")
+TUNE_H = os.path.join(CSRC, "tune_table.h")
+_PANEL = {"registers": 1, "half_shared": 2, 1: 1, 2: 2}
+
+
+def write_tune_header() -> str:
+    """csrc/tune_table.h from tune_table.json (rewritten only when it changes)."""
+    import json
+    with open(TUNE_JSON) as f:
+        t = json.load(f)
+    d = t["defaults"]
+    rows = []
+    for e in t["entries"]:
+        rows.append("    {%d, %d, %d, %d, %dLL, %dLL, %d, %d, %d},  // %s" % (
+            1 if e["dtype"] == "complex" else 0, 1 if e["mode"] == "split" else 0, e["n_min"], e["n_max"],
+            e["batch_min"], e["batch_max"], _PANEL[e["panel"]], e["slices"], e["ranges"],
+            e.get("note", "")))
+    body = "\n".join(rows) if rows else "    {-1, -1, 0, 0, 0LL, 0LL, 0, 0, 0},  // (no measured entries)"
+    text = f"""// tune_table.h -- generated by pfcuda_b200/build.py from pfcuda_b200/tune_table.json
+// (the table pfcuda_b200/tune.py measures); do not edit.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/pfb200.h"
+
+namespace pfb {{
+
+struct TuneEntry {{
+    int cplx, split, n_min, n_max;
+    long long batch_min, batch_max;
+    int panel, slices, ranges;
+}};
+
+static const TuneEntry kTuneTable[] = {{
+{body}
+}};
+
+// The first entry for this dtype class and mode whose order and batch bins
+// hold (n, batch), else the defaults.
+inline pfb_slog_config tuned_config(int dtype, int n, int64_t batch, bool split)
+{{
+    const int cplx = (dtype == PFB_C64 || dtype == PFB_C128) ? 1 : 0;
+    for (const TuneEntry &e : kTuneTable)
+        if (e.cplx == cplx && e.split == (split ? 1 : 0) && n >= e.n_min && n <= e.n_max &&
+            batch >= e.batch_min && batch <= e.batch_max)
+            return pfb_slog_config{{e.panel, e.slices, e.ranges}};
+    return pfb_slog_config{{{_PANEL[d["panel"]]}, {d["slices"]}, {d["ranges"]}}};
+}}
+
+}}  // namespace pfb
+"""
+    old = open(TUNE_H).read() if os.path.exists(TUNE_H) else None
+    if old != text:
+        with open(TUNE_H, "w") as f:
+            f.write(text)
+    return TUNE_H
+
+
 def _deps():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+        glob.glob(os.path.join(INCLUDE, "*.h"))
 
 
 def _compile(src, verbose):
@@ -46,6 +105,7 @@ def _compile(src, verbose):
 
 def build(verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
+    write_tune_header()
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         results = list(ex.map(lambda s: _compile(s, verbose), srcs))

@@ -74,13 +74,29 @@ int pfb_slog_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout
 int pfb_slog_max_concurrent(int dtype, int n)
 {
     if (!valid_dtype(dtype) || n <= 32) return 0;
-    return pfb::large_max_concurrent(dtype, n);
+    return pfb::large_max_concurrent(dtype, n, PFB_PANEL_REGISTERS);
 }
 
-int pfb_slog_stream_ranges(int dtype, int64_t batch, int n)
+int pfb_slog_max_concurrent_form(int dtype, int n, int panel)
 {
-    if (!valid_dtype(dtype) || batch <= 0 || n <= 32 || (n & 1)) return 1;
-    return pfb::large_second_range(dtype, batch, n) > 0 ? 2 : 1;
+    if (!valid_dtype(dtype) || n <= 32 || (panel != PFB_PANEL_REGISTERS && panel != PFB_PANEL_HALF_SHARED)) return 0;
+    pfb_slog_config over{panel, 0, 0}, cf;
+    if (!pfb::large_config(dtype, 1, n, PFB_MODE_FP64, &over, &cf)) return 0;
+    return pfb::large_max_concurrent(dtype, n, panel);
+}
+
+int pfb_slog_config_for(int dtype, int64_t batch, int n, int mode, pfb_slog_config *out)
+{
+    if (!valid_dtype(dtype) || batch < 0 || n < 0 || !out) return PFB_ERR_INVALID;
+    if (n <= 32 || (n & 1) || pfb::large_workspace_bytes(dtype, 1, n, mode) == 0) return PFB_ERR_SIZE;
+    return pfb::large_config(dtype, batch, n, mode, nullptr, out) ? PFB_OK : PFB_ERR_INVALID;
+}
+
+int pfb_slog_stream_ranges(int dtype, int64_t batch, int n, int mode)
+{
+    pfb_slog_config cf;
+    if (pfb_slog_config_for(dtype, batch, n, mode, &cf) != PFB_OK || batch <= 0) return 1;
+    return pfb::large_second_range(dtype, batch, n, cf) > 0 ? 2 : 1;
 }
 
 int pfb_slog_panel_width(int dtype, int n)
@@ -92,6 +108,14 @@ int pfb_slog_panel_width(int dtype, int n)
 int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                             double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
                             void *stream, const pfb_slog_timing *timing)
+{
+    return pfb_slog_pfaffian_ex(dtype, A, batch, n, layout, mode, log_out, sign_out, workspace, workspace_bytes,
+                                stream, timing, nullptr);
+}
+
+int pfb_slog_pfaffian_ex(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
+                         double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
+                         void *stream, const pfb_slog_timing *timing, const pfb_slog_config *config)
 {
     if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
     if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
@@ -109,7 +133,7 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
         if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u))
             return PFB_ERR_WORKSPACE;
         rc = pfb::launch_large(dtype, A, batch, n, layout, mode, log_out, sign_out, workspace,
-                               workspace_bytes, s, timing);
+                               workspace_bytes, s, timing, config);
     }
     if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
     return rc;

@@ -44,6 +44,7 @@
 #include "split.cuh"
 #include "panel.cuh"
 #include "dmma.cuh"
+#include "tune_table.h"
 
 namespace pfb {
 
@@ -148,6 +149,19 @@ panel_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all
     PanelSmem<T, NB> &sm = *reinterpret_cast<PanelSmem<T, NB> *>(smem_raw);
     const int64_t b = blockIdx.y;
     panel_body<T, NB, CPT>(sm, W_all + b * (int64_t)n * n, n, k0, st_all + b, piv_all + b * (int64_t)(n / 2));
+}
+
+// The same panel with half of each window in shared memory (panel_body_hs):
+// at most 128 registers per thread, so two CTAs fit on an SM.
+template <typename T, int NB>
+__global__ void __launch_bounds__(kTT, 2)
+panel_hs_kernel(T *__restrict__ W_all, int n, int k0, MatState *__restrict__ st_all,
+                int32_t *__restrict__ piv_all)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PanelSmemHS<T, NB> &sm = *reinterpret_cast<PanelSmemHS<T, NB> *>(smem_raw);
+    const int64_t b = blockIdx.y;
+    panel_body_hs<T, NB>(sm, W_all + b * (int64_t)n * n, n, k0, st_all + b, piv_all + b * (int64_t)(n / 2));
 }
 
 // The int8 operand images of the split update for the panel at k0 (a full
@@ -344,9 +358,8 @@ template <typename T, int NB, int CPT>
 // it (A, log_out and sign_out are already offset to matrix b0).
 static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_t B, int n, int layout,
                      int mode, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s,
-                     const pfb_slog_timing *tm)
+                     const pfb_slog_timing *tm, const pfb_slog_config &cf)
 {
-    using SM = PanelSmem<T, NB>;
     const LargeLayout L = large_layout(dtype, batch, n, mode);
     int32_t *piv = reinterpret_cast<int32_t *>(ws + L.piv_off) + b0 * (n / 2);
     MatState *st = reinterpret_cast<MatState *>(ws + L.st_off) + b0;
@@ -376,8 +389,16 @@ static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_
         if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
     }
 
-    auto pk = panel_kernel<T, NB, CPT>;
-    const size_t psmem = sizeof(SM);
+    // the panel form: the whole window in registers (one CTA per SM), or half
+    // of it in shared memory (two CTAs per SM; one trailing column per thread)
+    void (*pk)(T *, int, int, MatState *, int32_t *) = panel_kernel<T, NB, CPT>;
+    size_t psmem = sizeof(PanelSmem<T, NB>);
+    if constexpr (CPT == 1) {
+        if (cf.panel == PFB_PANEL_HALF_SHARED) {
+            pk = panel_hs_kernel<T, NB>;
+            psmem = sizeof(PanelSmemHS<T, NB>);
+        }
+    }
     if (cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) != cudaSuccess)
         return PFB_ERR_CUDA;
     if (cudaFuncSetAttribute(pk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -400,7 +421,7 @@ static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_
 
     SplitArgs sa{};
     unsigned char *split_ws = ws + L.split_off;
-    const int slices = ((mode >> 8) & 0xf) ? ((mode >> 8) & 0xf) : kSplitDefaultSlices;
+    const int slices = cf.slices;
     int32_t *split_err = nullptr;
     if ((mode & 0xff) == PFB_MODE_SPLIT) {
         split_err = split_args(true, split_ws, cplx, batch, n, NB, 0, slices).err + b0;
@@ -474,13 +495,19 @@ static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_
 }
 
 template <typename T, int NB, int CPT>
-static int max_concurrent_t(int n)
+static int max_concurrent_t(int n, int panel)
 {
     const int mt = n - NB;
     int CL = mt > 0 ? (mt + kTT * CPT - 1) / (kTT * CPT) : 1;
     if (CL < 1) CL = 1;
-    auto pk = panel_kernel<T, NB, CPT>;
-    const size_t psmem = sizeof(PanelSmem<T, NB>);
+    void (*pk)(T *, int, int, MatState *, int32_t *) = panel_kernel<T, NB, CPT>;
+    size_t psmem = sizeof(PanelSmem<T, NB>);
+    if constexpr (CPT == 1) {
+        if (panel == PFB_PANEL_HALF_SHARED) {
+            pk = panel_hs_kernel<T, NB>;
+            psmem = sizeof(PanelSmemHS<T, NB>);
+        }
+    }
     if (cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) != cudaSuccess) return 0;
     if (cudaFuncSetAttribute(pk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 0;
     cudaLaunchConfig_t cfg = {};
@@ -495,22 +522,30 @@ static int max_concurrent_t(int n)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int num = 0;
-    if (cudaOccupancyMaxActiveClusters(&num, pk, &cfg) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveClusters(&num, (const void *)pk, &cfg) != cudaSuccess) return 0;
     return num;
 }
 
-int large_max_concurrent(int dtype, int n)
+int large_max_concurrent(int dtype, int n, int panel)
 {
     int nb = 0, cpt = 0;
     if (!large_cfg(dtype, n, &nb, &cpt)) return 0;
     const bool cplx = dtype == PFB_C64 || dtype == PFB_C128;
-    if (!cplx) return nb == 64 ? max_concurrent_t<double, 64, 1>(n) : max_concurrent_t<double, 32, 2>(n);
-    return max_concurrent_t<c128, 32, 1>(n);
+    if (!cplx) return nb == 64 ? max_concurrent_t<double, 64, 1>(n, panel) : max_concurrent_t<double, 32, 2>(n, panel);
+    return max_concurrent_t<c128, 32, 1>(n, panel);
+}
+
+// Whether the half-shared panel form exists for this order (one trailing
+// column per thread).
+static bool hs_available(int dtype, int n)
+{
+    int nb = 0, cpt = 0;
+    return large_cfg(dtype, n, &nb, &cpt) && cpt == 1;
 }
 
 static int run_large_range(int dtype, const void *A, int64_t batch, int64_t b0, int64_t B, int n, int layout,
                            int mode, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s,
-                           const pfb_slog_timing *timing)
+                           const pfb_slog_timing *timing, const pfb_slog_config &cf)
 {
     int nb = 0, cpt = 0;
     large_cfg(dtype, n, &nb, &cpt);
@@ -521,10 +556,10 @@ static int run_large_range(int dtype, const void *A, int64_t batch, int64_t b0, 
     void *so = static_cast<char *>(sign_out) + (size_t)b0 * sign_es;
     const bool cplx = dtype == PFB_C64 || dtype == PFB_C128;
     if (!cplx) {
-        if (nb == 64) return run_large<double, 64, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing);
-        return run_large<double, 32, 2>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing);
+        if (nb == 64) return run_large<double, 64, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
+        return run_large<double, 32, 2>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
     }
-    return run_large<c128, 32, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing);
+    return run_large<c128, 32, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
 }
 
 // The second stream of this host thread's calls on device `dev`: one per thread
@@ -573,32 +608,62 @@ static bool aux_usable(cudaStream_t caller, cudaStream_t aux)
 // can be captured in a CUDA graph.  The second stream is this host thread's own
 // (aux_stream); when it is part of another capture the call runs as one range.
 //
-// The size of the second range (0: one range) for a call on `batch` matrices.
-int64_t large_second_range(int dtype, int64_t batch, int n)
+// The configuration of a call: the caller's fields where it gives them, else
+// the tuned table's choice for (dtype, n, batch) (tune_table.h, written by
+// pfcuda_b200/tune.py), else the defaults.  Returns false for an invalid
+// override.
+bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_config *over, pfb_slog_config *out)
+{
+    pfb_slog_config c = tuned_config(dtype, n, batch, (mode & 0xff) == PFB_MODE_SPLIT);
+    if (!hs_available(dtype, n)) c.panel = PFB_PANEL_REGISTERS;
+    if ((mode >> 8) & 0xf) c.slices = (mode >> 8) & 0xf;
+    if (over) {
+        if (over->panel < 0 || over->panel > 2 || over->slices < 0 || over->slices > kSplitMaxSlices ||
+            over->ranges < 0 || over->ranges > 2)
+            return false;
+        if (over->panel) {
+            if (over->panel == PFB_PANEL_HALF_SHARED && !hs_available(dtype, n)) return false;
+            c.panel = over->panel;
+        }
+        if (over->slices) c.slices = over->slices;
+        if (over->ranges) c.ranges = over->ranges;
+    }
+    *out = c;
+    return true;
+}
+
+// The size of the second range (0: one range) for a call on `batch` matrices:
+// the last wave's worth of the widest panel clusters, when the configuration
+// asks for two ranges and the batch holds three waves or more of clusters of
+// 9 or more CTAs.
+int64_t large_second_range(int dtype, int64_t batch, int n, const pfb_slog_config &cf)
 {
     int nb = 0, cpt = 0;
-    if (!large_cfg(dtype, n, &nb, &cpt)) return 0;
+    if (cf.ranges != 2 || !large_cfg(dtype, n, &nb, &cpt)) return 0;
     const int widest = (n - nb + kTT * cpt - 1) / (kTT * cpt);
     if (widest < 9) return 0;
-    const int mc = large_max_concurrent(dtype, n);
+    const int mc = large_max_concurrent(dtype, n, cf.panel);
     return (mc > 0 && batch >= 3 * (int64_t)mc) ? mc : 0;
 }
 
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
-                 cudaStream_t stream, const pfb_slog_timing *timing)
+                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *over)
 {
     int nb = 0, cpt = 0;
     if (!large_cfg(dtype, n, &nb, &cpt)) return PFB_ERR_SIZE;
     if ((mode & 0xff) == PFB_MODE_SPLIT && !split_available()) return PFB_ERR_UNSUPPORTED;
     if (batch > 65535) return PFB_ERR_SIZE;
+    pfb_slog_config cf;
+    if (!large_config(dtype, batch, n, mode, over, &cf)) return PFB_ERR_INVALID;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
-    const int64_t mc = timing == nullptr ? large_second_range(dtype, batch, n) : 0;
+    const int64_t mc = timing == nullptr ? large_second_range(dtype, batch, n, cf) : 0;
     int dev = 0;
     cudaStream_t s2 = nullptr;
     if (mc > 0 && cudaGetDevice(&dev) == cudaSuccess) s2 = aux_stream(dev);
     if (s2 && !aux_usable(stream, s2)) s2 = nullptr;
-    if (!s2) return run_large_range(dtype, A, batch, 0, batch, n, layout, mode, log_out, sign_out, ws, stream, timing);
+    if (!s2)
+        return run_large_range(dtype, A, batch, 0, batch, n, layout, mode, log_out, sign_out, ws, stream, timing, cf);
 
     const int64_t B2 = mc, B1 = batch - B2;
     cudaEvent_t fork, join;
@@ -611,11 +676,11 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
     if (cudaEventRecord(fork, stream) != cudaSuccess || cudaStreamWaitEvent(s2, fork, 0) != cudaSuccess)
         rc = PFB_ERR_CUDA;
     if (rc == PFB_OK)
-        rc = run_large_range(dtype, A, batch, 0, B1, n, layout, mode, log_out, sign_out, ws, stream, nullptr);
+        rc = run_large_range(dtype, A, batch, 0, B1, n, layout, mode, log_out, sign_out, ws, stream, nullptr, cf);
     // the second range always runs (or at least joins), so the fork is always closed
-    const int rc2 =
-        rc == PFB_OK ? run_large_range(dtype, A, batch, B1, B2, n, layout, mode, log_out, sign_out, ws, s2, nullptr)
-                     : PFB_OK;
+    const int rc2 = rc == PFB_OK ? run_large_range(dtype, A, batch, B1, B2, n, layout, mode, log_out, sign_out, ws,
+                                                   s2, nullptr, cf)
+                                 : PFB_OK;
     if (cudaEventRecord(join, s2) != cudaSuccess || cudaStreamWaitEvent(stream, join, 0) != cudaSuccess)
         rc = PFB_ERR_CUDA;
     cudaEventDestroy(fork);

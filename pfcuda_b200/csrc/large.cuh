@@ -22,11 +22,12 @@ size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode);
 
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
-                 cudaStream_t stream, const pfb_slog_timing *timing);
+                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *config = nullptr);
+bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_config *over, pfb_slog_config *out);
 
 int large_panel_width(int dtype, int n);
-int large_max_concurrent(int dtype, int n);
-int64_t large_second_range(int dtype, int64_t batch, int n);
+int large_max_concurrent(int dtype, int n, int panel);
+int64_t large_second_range(int dtype, int64_t batch, int n, const pfb_slog_config &cf);
 
 // Where the factorisation leaves its results inside a large-path workspace:
 // the pivot columns (n/2 per matrix), the per-matrix state, and W, the

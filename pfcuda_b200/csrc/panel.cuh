@@ -147,8 +147,8 @@ PFB_D void store_pair(c128 *p, c128 a, c128 b) { p[0] = a; p[1] = b; }
 // c_u = lb[2u][col], c_w = lb[2u+1][col].  Four partial sums shorten the
 // dependency chain; chunks of 8 pairs with a compiler barrier between them keep
 // the coefficient loads from all being hoisted into registers at once.
-template <typename T, int NB>
-PFB_D T lazy_row(T s, const T (&Rw)[NB], const T (*lb)[NB + 1], int col, int fin0)
+template <typename T, int NB, int LBW = NB>
+PFB_D T lazy_row(T s, const T (&Rw)[NB], const T (*lb)[LBW + 1], int col, int fin0)
 {
     T s2 = zero<T>(), s3 = zero<T>(), s4 = zero<T>();
 #pragma unroll
@@ -219,6 +219,157 @@ PFB_D c128 ld_remote(uint32_t addr, c128 *)
     return mk(re, im);
 }
 
+// Steps (2)-(4) of a pivot step, shared by both panel forms: this thread's
+// best candidate (key bits kb, column col, value val; `mine`: one of this
+// thread's trailing columns), the warp's best, the CTA's best -- whose header
+// goes to every CTA of the cluster, and which, if it is a trailing column, its
+// owner stages (stage()) -- the save of column k+1 for a trailing pivot's
+// owner, the group barrier, and the pivot: its value a, column j and the CTA
+// gs holding it.  Returns false for a zero pivot.
+template <typename T, int NB, bool SOLO, typename Stage>
+PFB_D bool pick_pivot(PanelSmem<T, NB> &sm, int t, int CL, uint32_t rank, bool has_panel, unsigned long long kb,
+                      int col, T val, bool mine, Stage &&stage, T &a, int &j, int &gs)
+{
+    constexpr int NW = PanelSmem<T, NB>::NW;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int par = t & 1;
+    unsigned long long wk;
+    int wc;
+    warp_argmax(kb, col, wk, wc);
+    if (wc != INT_MAX && col == wc) sm.wval[warp] = val;
+    if (lane == 0) { sm.wkey[warp] = wk; sm.wcol[warp] = wc; }
+    __syncthreads();
+
+    // (3) the CTA's best candidate: its header goes to every CTA of the
+    // cluster, and if it is a trailing column its owner stages the column
+    // (the same warp reductions over the NW warp results, lane w reading warp w's)
+    const unsigned long long wkl = lane < NW ? sm.wkey[lane] : 0ull;
+    const int wcl = lane < NW ? sm.wcol[lane] : INT_MAX;
+    unsigned long long ck;
+    int cc;
+    warp_argmax(wkl, wcl, ck, cc);
+    int cw = __ffs(__ballot_sync(0xffffffffu, lane < NW && wcl == cc && wkl == ck)) - 1;
+    cw = cw < 0 ? 0 : cw;
+    // (a CTA without candidates sends key 0 and column INT_MAX)
+    if (tid < CL)
+        put_hdr(map_rank(smem_u32(&sm.hdr[par][rank]), tid), cc == INT_MAX ? zero<T>() : sm.wval[cw], cc);
+    if (mine && col == cc) stage();
+    // if the pivot column is a trailing one, its owner fills its window
+    // from column k+1 of the panel rows above k+1 and the negated row k+1
+    // right of it: saved here, so that (5) can overwrite them in lb
+    // without a barrier between the owner's reads and those writes
+    if (has_panel) {
+        const int x = tid;
+        sm.k1col[par][x] = (x <= 2 * t) ? sm.lb[x][2 * t + 1]
+                                        : ((x > 2 * t + 1) ? neg(sm.lb[2 * t + 1][x]) : zero<T>());
+    }
+    group_sync<SOLO>();
+
+    // (4) the pivot: the first maximum over the CL <= 16 headers, lane s of
+    // every warp reading header s
+    T hv = zero<T>();
+    int hc = INT_MAX;
+    if (lane < CL) { hv = sm.hdr[par][lane].val; hc = sm.hdr[par][lane].col; }
+    unsigned long long hk;
+    warp_argmax(lane < CL ? key_bits(pkey(hv)) : 0ull, hc, hk, j);
+    gs = __ffs(__ballot_sync(0xffffffffu, lane < CL && hc == j)) - 1;
+    a = shfl(hv, gs);
+    return !(is_zero(a) || j == INT_MAX);
+}
+
+// The panel-column part of the interchange k+1 <-> j (k = k0 + 2t, jl = j - k0):
+// panel thread x reads the lb entries it will move (read_*), then writes them
+// back permuted (write).  Thread x touches only row x and column x of lb.
+template <typename T>
+struct LbSwap {
+    T tI = zero<T>(), tJ = zero<T>(), tRi = zero<T>(), tRj = zero<T>();
+
+    // j is a panel column
+    template <int NB>
+    PFB_D void read_in_panel(const PanelSmem<T, NB> &sm, int t, int jl)
+    {
+        const int x = threadIdx.x;
+        if (x <= 2 * t) { tI = sm.lb[x][2 * t + 1]; tJ = sm.lb[x][jl]; }
+        if (x > 2 * t + 1 && x < jl) { tJ = sm.lb[x][jl]; tRi = sm.lb[2 * t + 1][x]; }
+        if (x == jl) tRi = sm.lb[2 * t + 1][jl];
+        if (x > jl) { tRi = sm.lb[2 * t + 1][x]; tRj = sm.lb[jl][x]; }
+    }
+    // j is a trailing column: its panel entries come from the stage of CTA gs
+    template <int NB>
+    PFB_D void read_trailing(PanelSmem<T, NB> &sm, int t, int gs)
+    {
+        tJ = ld_remote(map_rank(smem_u32(&sm.stage[t & 1][threadIdx.x]), (uint32_t)gs), (T *)nullptr);
+    }
+    template <int NB>
+    PFB_D void write(PanelSmem<T, NB> &sm, int t, int jl, bool trail_win) const
+    {
+        const int x = threadIdx.x;
+        if (!trail_win) {
+            if (x <= 2 * t) { sm.lb[x][2 * t + 1] = tJ; sm.lb[x][jl] = tI; }
+            if (x > 2 * t + 1 && x < jl) { sm.lb[2 * t + 1][x] = neg(tJ); sm.lb[x][jl] = neg(tRi); }
+            if (x == jl) sm.lb[2 * t + 1][jl] = neg(tRi);
+            if (x > jl) { sm.lb[2 * t + 1][x] = tRj; sm.lb[jl][x] = tRi; }
+        } else {
+            if (x <= 2 * t) sm.lb[x][2 * t + 1] = tJ;
+            if (x > 2 * t + 1) sm.lb[2 * t + 1][x] = neg(tJ);
+        }
+    }
+};
+
+// This panel's pivots (t <= NB/2 <= 32 of them): lane s of warp 0 of rank 0
+// records pivot column s and takes pivot s, then one warp tree sums the logs
+// and multiplies the phases into the leader's running (la, pre + i pim).
+template <typename T, int NB>
+PFB_D void panel_log_pivots(const PanelSmem<T, NB> &sm, int t, int k0, uint32_t rank, bool leader,
+                            int32_t *__restrict__ piv, double &la, double &pre, double &pim)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (rank != 0 || warp != 0) return;
+    double lg = 0.0, ar = 1.0, ai = 0.0;
+    if (lane < t) {
+        const T a = sm.pivval[lane];
+        piv[k0 / 2 + lane] = sm.pivcol[lane];
+        const double m = (double)mag(a);
+        lg = log(m);
+        if constexpr (IsComplex<T>::value) { ar = a.re / m; ai = a.im / m; }
+        else { ar = a < 0 ? -1.0 : 1.0; }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        lg += shfl_xor(lg, off);
+        const double br = shfl_xor(ar, off), bi = shfl_xor(ai, off);
+        const double nr = ar * br - ai * bi, ni = ar * bi + ai * br;
+        ar = nr;
+        ai = ni;
+    }
+    if (leader) {
+        la += lg;
+        const double nr = pre * ar - pim * ai, ni = pre * ai + pim * ar;
+        pre = nr;
+        pim = ni;
+    }
+}
+
+// The factored NB x NB panel block (strict upper part) back to W, by rank 0.
+template <typename T, int NB>
+PFB_D void panel_store_block(const PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, uint32_t rank, int pc)
+{
+    const int tid = threadIdx.x;
+    if (tid < NB && rank == 0 && pc < n)
+        for (int r = 0; r < NB && r < tid; r++) W[(int64_t)(k0 + r) * n + pc] = sm.lb[r][tid];
+}
+
+PFB_D void panel_save_state(MatState *__restrict__ st, bool leader, double la, double pre, double pim, int parity)
+{
+    if (!leader) return;
+    // keep the phase on the unit circle across panels
+    const double m = sqrt(pre * pre + pim * pim);
+    st->log_abs = la;
+    st->ph_re = pre / m;
+    st->ph_im = pim / m;
+    st->parity = parity;
+}
+
 // Factor panel rows [k0, k0+NB) of every matrix; one cluster of CL CTAs per
 // matrix (blockIdx.y).  Thread i of CTA rank r keeps trailing columns
 // k0+NB + r*kTT + i + q*CL*kTT (q < CPT) of the panel rows in registers; threads
@@ -241,13 +392,7 @@ template <typename T, int NB, int CPT, bool SOLO = false>
 PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, MatState *__restrict__ st,
                       int32_t *__restrict__ piv)
 {
-    using Real = typename RealOf<T>::type;
-    using SM = PanelSmem<T, NB>;
-    constexpr int NW = SM::NW;
-
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
     const bool has_panel = tid < NB;
     const uint32_t rank = cluster_rank();
     const int CL = (int)cluster_size();
@@ -321,27 +466,8 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                 if (kq > kb || col == INT_MAX) { kb = kq; col = cq[q]; qsel = q; val = Rw[q][0]; }
             }
         }
-        unsigned long long wk;
-        int wc;
-        warp_argmax(kb, col, wk, wc);
-        if (wc != INT_MAX && col == wc) sm.wval[warp] = val;
-        if (lane == 0) { sm.wkey[warp] = wk; sm.wcol[warp] = wc; }
-        __syncthreads();
-
-        // (3) the CTA's best candidate: its header goes to every CTA of the
-        // cluster, and if it is a trailing column its owner stages the column
-        // (the same warp reductions over the NW warp results, lane w reading warp w's)
-        const unsigned long long wkl = lane < NW ? sm.wkey[lane] : 0ull;
-        const int wcl = lane < NW ? sm.wcol[lane] : INT_MAX;
-        unsigned long long ck;
-        int cc;
-        warp_argmax(wkl, wcl, ck, cc);
-        int cw = __ffs(__ballot_sync(0xffffffffu, lane < NW && wcl == cc && wkl == ck)) - 1;
-        cw = cw < 0 ? 0 : cw;
-        // (a CTA without candidates sends key 0 and column INT_MAX)
-        if (tid < CL)
-            put_hdr(map_rank(smem_u32(&sm.hdr[par][rank]), tid), cc == INT_MAX ? zero<T>() : sm.wval[cw], cc);
-        if (qsel >= 0 && col == cc) {
+        // the owner of the CTA's best trailing column stages its NB panel entries
+        auto stage = [&]() {
 #pragma unroll
             for (int P = 0; P < NB / 2; P++) {
                 // window pair P holds panel rows (r, r+1), r even
@@ -354,29 +480,13 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                 }
                 store_pair(&sm.stage[par][r], v0, v1);
             }
+        };
+        T a;
+        int j, gs;
+        if (!pick_pivot<T, NB, SOLO>(sm, t, CL, rank, has_panel, kb, col, val, qsel >= 0, stage, a, j, gs)) {
+            dead = true;
+            break;
         }
-        // if the pivot column is a trailing one, its owner fills its window
-        // from column k+1 of the panel rows above k+1 and the negated row k+1
-        // right of it: saved here, so that (5) can overwrite them in lb
-        // without a barrier between the owner's reads and those writes
-        if (has_panel) {
-            const int x = tid;
-            sm.k1col[par][x] = (x <= 2 * t) ? sm.lb[x][2 * t + 1]
-                                            : ((x > 2 * t + 1) ? neg(sm.lb[2 * t + 1][x]) : zero<T>());
-        }
-        group_sync<SOLO>();
-
-        // (4) the pivot: the first maximum over the CL <= 16 headers, lane s of
-        // every warp reading header s
-        T hv = zero<T>();
-        int hc = INT_MAX;
-        if (lane < CL) { hv = sm.hdr[par][lane].val; hc = sm.hdr[par][lane].col; }
-        unsigned long long hk;
-        int j;
-        warp_argmax(lane < CL ? key_bits(pkey(hv)) : 0ull, hc, hk, j);
-        const int gs = __ffs(__ballot_sync(0xffffffffu, lane < CL && hc == j)) - 1;
-        const T a = shfl(hv, gs);
-        if (is_zero(a) || j == INT_MAX) { dead = true; break; }
 
         // (5) interchange k+1 <-> j on the upper triangle.  The trailing rows'
         // entries come from global memory; their loads are issued here and
@@ -392,7 +502,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         if (j != k + 1) {
             const int jl = j - k0;
             const bool trail_win = j >= k1;
-            T tI = zero<T>(), tJ = zero<T>(), tRi = zero<T>(), tRj = zero<T>();
+            LbSwap<T> lbx;
             if (!trail_win) {
                 // rows k+1 (position 1) and j (position jl - 2t) of every
                 // trailing column: row j moves up now, row k+1 down in (7)
@@ -402,13 +512,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                     r1s[q] = Rw[q][1];
                     Rw[q][1] = window_row<T, NB>(Rw[q], qswap);
                 }
-                if (has_panel) {
-                    const int x = tid;
-                    if (x <= 2 * t) { tI = sm.lb[x][2 * t + 1]; tJ = sm.lb[x][jl]; }
-                    if (x > 2 * t + 1 && x < jl) { tJ = sm.lb[x][jl]; tRi = sm.lb[2 * t + 1][x]; }
-                    if (x == jl) tRi = sm.lb[2 * t + 1][jl];
-                    if (x > jl) { tRi = sm.lb[2 * t + 1][x]; tRj = sm.lb[jl][x]; }
-                }
+                if (has_panel) lbx.read_in_panel(sm, t, jl);
             } else {
 #pragma unroll
                 for (int q = 0; q < CPT; q++) {
@@ -432,24 +536,12 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
                         guse[q] = true;
                     }
                 }
-                if (has_panel)
-                    tJ = ld_remote(map_rank(smem_u32(&sm.stage[par][tid]), (uint32_t)gs), (T *)nullptr);
+                if (has_panel) lbx.read_trailing(sm, t, gs);
             }
             // no barrier here: every lb entry below is read above by the thread
             // that writes it (panel thread x reads and writes only lb[x][.] and
             // lb[.][x]), and the trailing owner of column j read k1col instead
-            if (has_panel) {
-                const int x = tid;
-                if (!trail_win) {
-                    if (x <= 2 * t) { sm.lb[x][2 * t + 1] = tJ; sm.lb[x][jl] = tI; }
-                    if (x > 2 * t + 1 && x < jl) { sm.lb[2 * t + 1][x] = neg(tJ); sm.lb[x][jl] = neg(tRi); }
-                    if (x == jl) sm.lb[2 * t + 1][jl] = neg(tRi);
-                    if (x > jl) { sm.lb[2 * t + 1][x] = tRj; sm.lb[jl][x] = tRi; }
-                } else {
-                    if (x <= 2 * t) sm.lb[x][2 * t + 1] = tJ;
-                    if (x > 2 * t + 1) sm.lb[2 * t + 1][x] = neg(tJ);
-                }
-            }
+            if (has_panel) lbx.write(sm, t, jl, trail_win);
             __syncthreads();
             parity ^= 1;
         }
@@ -498,33 +590,7 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
         group_sync<SOLO>();
         return;
     }
-    // this panel's pivots (t <= NB/2 <= 32): lane s of warp 0 of rank 0 takes
-    // pivot s, then one warp tree sums the logs and multiplies the phases
-    if (rank == 0 && warp == 0) {
-        double lg = 0.0, ar = 1.0, ai = 0.0;
-        if (lane < t) {
-            const T a = sm.pivval[lane];
-            piv[k0 / 2 + lane] = sm.pivcol[lane];
-            const double m = (double)mag(a);
-            lg = log(m);
-            if constexpr (IsComplex<T>::value) { ar = a.re / m; ai = a.im / m; }
-            else { ar = a < 0 ? -1.0 : 1.0; }
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            lg += shfl_xor(lg, off);
-            const double br = shfl_xor(ar, off), bi = shfl_xor(ai, off);
-            const double nr = ar * br - ai * bi, ni = ar * bi + ai * br;
-            ar = nr;
-            ai = ni;
-        }
-        if (leader) {
-            la += lg;
-            const double nr = pre * ar - pim * ai, ni = pre * ai + pim * ar;
-            pre = nr;
-            pim = ni;
-        }
-    }
+    panel_log_pivots(sm, t, k0, rank, leader, piv, la, pre, pim);
 
     // ---- write the factored panel rows back (t steps done: window position p
     // holds panel row 2t+p for p < NB-2t, else row p-(NB-2t))
@@ -535,17 +601,337 @@ PFB_D void panel_body(PanelSmem<T, NB> &sm, T *__restrict__ W, int n, int k0, Ma
             const int r = (p < NB - 2 * t) ? 2 * t + p : p - (NB - 2 * t);
             if (cq[q] < n && k0 + r < n) W[(int64_t)(k0 + r) * n + cq[q]] = Rw[q][p];
         }
-    if (has_panel && rank == 0 && pc < n) {
-        for (int r = 0; r < NB && r < tid; r++) W[(int64_t)(k0 + r) * n + pc] = sm.lb[r][tid];
+    panel_store_block(sm, W, n, k0, rank, pc);
+    panel_save_state(st, leader, la, pre, pim, parity);
+    group_sync<SOLO>();
+}
+
+
+// ------------------------------------------- panel with half a window in smem
+
+// The shared memory of panel_body_hs: PanelSmem plus rows NB/2 .. NB-1 of every
+// trailing column's window, one column per thread (sw[r][thread]: the threads
+// of a warp touch consecutive words).
+template <typename T, int NB>
+struct PanelSmemHS {
+    PanelSmem<T, NB> base;
+    alignas(16) T sw[NB / 2][kTT];
+};
+
+// The lazy sum of panel_body_hs's second phase: s + the Gauss-vector pairs
+// u < NB/4 (registers, window position p = panel row p) and NB/4 <= u < t
+// (sw), each  lb[2u][col] * w_u - lb[2u+1][col] * u_u  at this thread's column.
+// The pairs go into the same four partial sums, in the same order, as in
+// lazy_row over panel_body's window (pair u sits at window pair index
+// P = u + NB/2 - t there, and P odd feeds the sums that start from s), so both
+// panel forms round identically.
+template <typename T, int NB>
+PFB_D T lazy_mixed(T s, const T (&Rw)[NB / 2], const T (*sw)[kTT], const T (*lb)[NB + 1], int col, int t)
+{
+    constexpr int NR = NB / 2;
+    const int x = threadIdx.x;
+    const bool todd = t & 1;
+    // e: pairs with u even, o: u odd; the (u + t)-odd pair of sums starts from s
+    T e1 = todd ? s : zero<T>(), e2 = zero<T>();
+    T o1 = todd ? zero<T>() : s, o2 = zero<T>();
+#pragma unroll
+    for (int u = 0; u < NR / 2; u += 2) {
+        e1 = fma_(lb[2 * u][col], Rw[2 * u + 1], e1);
+        e2 = fms_(lb[2 * u + 1][col], Rw[2 * u], e2);
+        o1 = fma_(lb[2 * u + 2][col], Rw[2 * u + 3], o1);
+        o2 = fms_(lb[2 * u + 3][col], Rw[2 * u + 2], o2);
     }
+    int u = NR / 2;   // even
+#pragma unroll 1
+    for (; u + 1 < t; u += 2) {
+        e1 = fma_(lb[2 * u][col], sw[2 * u + 1 - NR][x], e1);
+        e2 = fms_(lb[2 * u + 1][col], sw[2 * u - NR][x], e2);
+        o1 = fma_(lb[2 * u + 2][col], sw[2 * u + 3 - NR][x], o1);
+        o2 = fms_(lb[2 * u + 3][col], sw[2 * u + 2 - NR][x], o2);
+    }
+    if (u < t) {
+        e1 = fma_(lb[2 * u][col], sw[2 * u + 1 - NR][x], e1);
+        e2 = fms_(lb[2 * u + 1][col], sw[2 * u - NR][x], e2);
+    }
+    return todd ? (e1 + e2) + (o1 + o2) : (o1 + o2) + (e1 + e2);
+}
+
+// panel_body for one trailing column per thread, with rows 0 .. NB/2-1 of the
+// column's window in registers and rows NB/2 .. NB-1 in shared memory (sw):
+// half the registers of panel_body's window, so two CTAs share an SM and twice
+// as many panel clusters run at once (the pivot steps are latency-bound, so two
+// CTAs interleave on one SM at little cost to either).  Same algorithm, same
+// pivots and the same rounding as panel_body.
+//   phase 1 (t < NB/4): the pivot rows come from the registers, which rotate as
+//     in panel_body (position p = row 2t+p for p < NB/2-2t, else row
+//     p-(NB/2-2t)); sw holds raw rows, and an interchange with a row there
+//     swaps it with row k+1 at once;
+//   phase 2: the registers hold the Gauss vectors of pairs 0 .. NB/4-1 in
+//     natural order (position p = row p); rows k, k+1 and the later pairs are
+//     read and written in sw in place, nothing rotates.
+template <typename T, int NB, bool SOLO = false>
+PFB_D void panel_body_hs(PanelSmemHS<T, NB> &smh, T *__restrict__ W, int n, int k0, MatState *__restrict__ st,
+                         int32_t *__restrict__ piv)
+{
+    constexpr int NR = NB / 2;   // window rows in registers
+    static_assert(NR % 4 == 0, "pairs of pairs in the register half");
+    PanelSmem<T, NB> &sm = smh.base;
+    T (*sw)[kTT] = smh.sw;
+    const int tid = threadIdx.x;
+    const bool has_panel = tid < NB;
+    const uint32_t rank = cluster_rank();
+    const int CL = (int)cluster_size();
+
+    if (st->dead) return;   // same value for the whole cluster
+
+    const int k1 = k0 + NB;
+    const int pc = k0 + tid;                      // panel column of this thread (if has_panel)
+    const int cq = k1 + (int)rank * kTT + tid;    // trailing column of this thread
+    const bool own = cq < n;
+
+    T Rw[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) Rw[r] = (own && k0 + r < n) ? W[(int64_t)(k0 + r) * n + cq] : zero<T>();
+#pragma unroll 4
+    for (int r = NR; r < NB; r++) sw[r - NR][tid] = (own && k0 + r < n) ? W[(int64_t)(k0 + r) * n + cq] : zero<T>();
+    if (has_panel) {
+        for (int r = 0; r < NB; r++)
+            sm.lb[r][tid] = (k0 + r < n && pc < n) ? W[(int64_t)(k0 + r) * n + pc] : zero<T>();
+    }
+
+    double la = 0.0, pre = 1.0, pim = 0.0;
+    int parity = 0;
+    const bool leader = rank == 0 && tid == 0;
     if (leader) {
-        // keep the phase on the unit circle across panels
-        const double m = sqrt(pre * pre + pim * pim);
-        st->log_abs = la;
-        st->ph_re = pre / m;
-        st->ph_im = pim / m;
-        st->parity = parity;
+        la = st->log_abs;
+        pre = st->ph_re;
+        pim = st->ph_im;
+        parity = st->parity;
     }
+    bool dead = false;
+    const int nsteps = (n - k0) / 2 < NB / 2 ? (n - k0) / 2 : NB / 2;
+    group_sync<SOLO>();
+
+    // a panel-column candidate (the smaller index) first, then the trailing one
+    auto panel_candidate = [&](int t, unsigned long long &kb, int &col, T &val) {
+        if (has_panel && tid > 2 * t && pc < n) {
+            const T s = lazy_panel<T, NB>(sm.lb, sm.lb[2 * t][tid], 2 * t, tid, t);
+            sm.lb[2 * t][tid] = s;
+            kb = key_bits(pkey(s));
+            col = pc;
+            val = s;
+        }
+    };
+    auto panel_finish = [&](int t, T a, int j, T ia) {
+        if (has_panel && tid > 2 * t + 1 && pc < n) {
+            const T s = lazy_panel<T, NB>(sm.lb, sm.lb[2 * t + 1][tid], 2 * t + 1, tid, t);
+            sm.lb[2 * t + 1][tid] = neg(s);
+            sm.lb[2 * t][tid] = sm.lb[2 * t][tid] * ia;
+        }
+        if (tid == 0) {
+            sm.pivval[t] = a;
+            sm.pivcol[t] = j;
+        }
+    };
+
+    int t = 0;
+    // ---- phase 1
+#pragma unroll 1
+    for (; t < nsteps && t < NR / 2; t++) {
+        const int k = k0 + 2 * t;
+        const int par = t & 1;
+        const int fin0 = NR / 2 - t;
+
+        Rw[0] = lazy_row<T, NR, NB>(Rw[0], Rw, sm.lb, 2 * t, fin0);
+        unsigned long long kb = 0;
+        int col = INT_MAX;
+        T val = zero<T>();
+        panel_candidate(t, kb, col, val);
+        bool mine = false;
+        if (own) {
+            const unsigned long long kq = key_bits(pkey(Rw[0]));
+            if (kq > kb || col == INT_MAX) { kb = kq; col = cq; mine = true; val = Rw[0]; }
+        }
+        auto stage = [&]() {
+#pragma unroll
+            for (int P = 0; P < NR / 2; P++) {
+                const int r = (2 * P < NR - 2 * t) ? 2 * t + 2 * P : 2 * P - (NR - 2 * t);
+                store_pair(&sm.stage[par][r], Rw[2 * P], Rw[2 * P + 1]);
+            }
+#pragma unroll 4
+            for (int r = NR; r < NB; r += 2) store_pair(&sm.stage[par][r], sw[r - NR][tid], sw[r + 1 - NR][tid]);
+        };
+        T a;
+        int j, gs;
+        if (!pick_pivot<T, NB, SOLO>(sm, t, CL, rank, has_panel, kb, col, val, mine, stage, a, j, gs)) {
+            dead = true;
+            break;
+        }
+
+        T gl = zero<T>(), r1s = zero<T>();
+        bool gneg = false, guse = false;
+        int qswap = -1;
+        if (j != k + 1) {
+            const int jl = j - k0;
+            const bool trail_win = j >= k1;
+            LbSwap<T> lbx;
+            if (!trail_win) {
+                if (jl < NR) {
+                    // row j at register position jl - 2t moves up now, row k+1 down in the rotation
+                    qswap = jl - 2 * t;
+                    r1s = Rw[1];
+                    Rw[1] = window_row<T, NR>(Rw, qswap);
+                } else {
+                    const T x = sw[jl - NR][tid];
+                    sw[jl - NR][tid] = Rw[1];
+                    Rw[1] = x;
+                }
+                if (has_panel) lbx.read_in_panel(sm, t, jl);
+            } else {
+                if (cq == j) {
+                    // the new column j: rows < k+1 from column k+1, (k+1, j)
+                    // negated, rows > k+1 (all of sw) from row k+1 negated
+#pragma unroll
+                    for (int p = 0; p < NR; p++) {
+                        const int r = (p < NR - 2 * t) ? 2 * t + p : p - (NR - 2 * t);
+                        if (p == 1) Rw[1] = neg(Rw[1]);
+                        else Rw[p] = sm.k1col[par][r];
+                    }
+#pragma unroll 4
+                    for (int r = NR; r < NB; r++) sw[r - NR][tid] = sm.k1col[par][r];
+                } else if (own) {
+                    const T *pp = (cq < j) ? &W[(int64_t)cq * n + j] : &W[(int64_t)j * n + cq];
+                    gl = ldcg(pp);
+                    gneg = cq < j;
+                    guse = true;
+                }
+                if (has_panel) lbx.read_trailing(sm, t, gs);
+            }
+            if (has_panel) lbx.write(sm, t, jl, trail_win);
+            __syncthreads();
+            parity ^= 1;
+        }
+
+        const T ia = recip(a);
+        T s1 = lazy_row<T, NR, NB>(guse ? zero<T>() : Rw[1], Rw, sm.lb, 2 * t + 1, fin0);
+        if (guse) {
+            s1 = s1 + (gneg ? neg(gl) : gl);
+            T *pp = (cq < j) ? &W[(int64_t)cq * n + j] : &W[(int64_t)j * n + cq];
+            stcg(pp, gneg ? neg(Rw[1]) : Rw[1]);
+        }
+        Rw[1] = neg(s1);
+        Rw[0] = Rw[0] * ia;
+        panel_finish(t, a, j, ia);
+
+        // rotate the register window; the old row k+1 lands where row j was
+        {
+            const T r0 = Rw[0], r1 = Rw[1];
+#pragma unroll
+            for (int p = 0; p < NR - 2; p++) Rw[p] = (p + 2 == qswap) ? r1s : Rw[p + 2];
+            Rw[NR - 2] = r0;
+            Rw[NR - 1] = r1;
+        }
+        __syncthreads();
+    }
+
+    // ---- phase 2
+#pragma unroll 1
+    for (; !dead && t < nsteps; t++) {
+        const int k = k0 + 2 * t;
+        const int par = t & 1;
+        const int s0 = 2 * t - NR, s1 = s0 + 1;   // sw rows of k and k+1
+
+        const T rk = lazy_mixed<T, NB>(sw[s0][tid], Rw, sw, sm.lb, 2 * t, t);
+        sw[s0][tid] = rk;
+        unsigned long long kb = 0;
+        int col = INT_MAX;
+        T val = zero<T>();
+        panel_candidate(t, kb, col, val);
+        bool mine = false;
+        if (own) {
+            const unsigned long long kq = key_bits(pkey(rk));
+            if (kq > kb || col == INT_MAX) { kb = kq; col = cq; mine = true; val = rk; }
+        }
+        auto stage = [&]() {
+#pragma unroll
+            for (int P = 0; P < NR / 2; P++) store_pair(&sm.stage[par][2 * P], Rw[2 * P], Rw[2 * P + 1]);
+#pragma unroll 4
+            for (int r = NR; r < NB; r += 2) store_pair(&sm.stage[par][r], sw[r - NR][tid], sw[r + 1 - NR][tid]);
+        };
+        T a;
+        int j, gs;
+        if (!pick_pivot<T, NB, SOLO>(sm, t, CL, rank, has_panel, kb, col, val, mine, stage, a, j, gs)) {
+            dead = true;
+            break;
+        }
+
+        T gl = zero<T>();
+        bool gneg = false, guse = false;
+        if (j != k + 1) {
+            const int jl = j - k0;
+            const bool trail_win = j >= k1;
+            LbSwap<T> lbx;
+            if (!trail_win) {
+                const T x = sw[jl - NR][tid];
+                sw[jl - NR][tid] = sw[s1][tid];
+                sw[s1][tid] = x;
+                if (has_panel) lbx.read_in_panel(sm, t, jl);
+            } else {
+                if (cq == j) {
+#pragma unroll
+                    for (int p = 0; p < NR; p++) Rw[p] = sm.k1col[par][p];
+#pragma unroll 4
+                    for (int r = NR; r < NB; r++)
+                        sw[r - NR][tid] = (r == 2 * t + 1) ? neg(sw[r - NR][tid]) : sm.k1col[par][r];
+                } else if (own) {
+                    const T *pp = (cq < j) ? &W[(int64_t)cq * n + j] : &W[(int64_t)j * n + cq];
+                    gl = ldcg(pp);
+                    gneg = cq < j;
+                    guse = true;
+                }
+                if (has_panel) lbx.read_trailing(sm, t, gs);
+            }
+            if (has_panel) lbx.write(sm, t, jl, trail_win);
+            __syncthreads();
+            parity ^= 1;
+        }
+
+        const T ia = recip(a);
+        const T raw1 = sw[s1][tid];
+        T v1 = lazy_mixed<T, NB>(guse ? zero<T>() : raw1, Rw, sw, sm.lb, 2 * t + 1, t);
+        if (guse) {
+            v1 = v1 + (gneg ? neg(gl) : gl);
+            T *pp = (cq < j) ? &W[(int64_t)cq * n + j] : &W[(int64_t)j * n + cq];
+            stcg(pp, gneg ? neg(raw1) : raw1);
+        }
+        sw[s1][tid] = neg(v1);
+        sw[s0][tid] = sw[s0][tid] * ia;
+        panel_finish(t, a, j, ia);
+        __syncthreads();
+    }
+
+    if (dead) {
+        if (leader) st->dead = 1;
+        group_sync<SOLO>();
+        return;
+    }
+    panel_log_pivots(sm, t, k0, rank, leader, piv, la, pre, pim);
+
+    // ---- write the factored panel rows back: registers in the phase-1
+    // arrangement if the panel ended there (t <= NB/4), else in natural order
+    if (own) {
+        const int tr = t < NR / 2 ? t : NR / 2;
+#pragma unroll
+        for (int p = 0; p < NR; p++) {
+            const int r = (p < NR - 2 * tr) ? 2 * tr + p : p - (NR - 2 * tr);
+            if (k0 + r < n) W[(int64_t)(k0 + r) * n + cq] = Rw[p];
+        }
+#pragma unroll 4
+        for (int r = NR; r < NB; r++)
+            if (k0 + r < n) W[(int64_t)(k0 + r) * n + cq] = sw[r - NR][tid];
+    }
+    panel_store_block(sm, W, n, k0, rank, pc);
+    panel_save_state(st, leader, la, pre, pim, parity);
     group_sync<SOLO>();
 }
 

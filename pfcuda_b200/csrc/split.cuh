@@ -12,7 +12,6 @@ namespace pfb {
 struct MatState;
 
 constexpr int kSplitMaxSlices = 7;
-constexpr int kSplitDefaultSlices = 7;
 constexpr int kSplitTileM = 128;   // rows of an operand chunk (the MMA M)
 
 // Everything the panel kernel needs to write the int8 operands of the update.

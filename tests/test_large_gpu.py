@@ -213,8 +213,9 @@ def test_two_stream_batches_match_single_ranges(mode):
     assert mc > 0
     B = 3 * mc
     # the call under test does run as two ranges, and a one-wave call as one
-    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n) == 2
-    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, mc, n) == 1
+    m = _lib.MODE_SPLIT if mode == "split" else _lib.MODE_FP64
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n, m) == 2
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, mc, n, m) == 1
     rng = np.random.default_rng(77)
     A = O.skew_normal(rng, B, n, scale=1 / np.sqrt(n))
     At = cuda(A)
@@ -232,7 +233,7 @@ def _two_range_batch(seed):
     n = 2176
     mc = _lib.lib().pfb_slog_max_concurrent(_lib.F64, n)
     B = 3 * mc
-    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n) == 2
+    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n, _lib.MODE_SPLIT) == 2
     rng = np.random.default_rng(seed)
     return cuda(O.skew_normal(rng, B, n, scale=1 / np.sqrt(n)))
 
