@@ -234,6 +234,64 @@ def measure_peaks(torch, dev, stream):
     return out
 
 
+def reference_gpu_baseline(torch, pf, _lib, O, dev, stream):
+    """The reference's own CUDA kernels on this GPU (src/*.cu compiled unchanged
+    for sm_100a into oracle/_ref/libref_gpu.so, driven the way its XLA handlers
+    drive them, bindings/jax_bindings.cu:19-112), beside this engine on the same
+    inputs: pf_sm_calc launched once per matrix on the 4096 x 32x32 float64
+    batch (jax_bindings.cu:107-109), and the host-driven slog_pfaffian_lg
+    (src/slog_pfaffian_lg.cu:151-211) on one matrix of order 1024 and 2048.
+    A reported baseline, like cpu_baseline: no engine number comes from it."""
+    import ctypes
+    if not os.path.exists(O.REF_GPU_SO):
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built"}
+    R = ctypes.CDLL(O.REF_GPU_SO)
+    R.refgpu_pfaffian_f64.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+    R.refgpu_slog_f64.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    out = {}
+    # the small path: the reference takes column-major matrices (pfcuda/cuda_api.py:50)
+    Ah = O.config_small()
+    Acm = torch.from_numpy(np.ascontiguousarray(np.swapaxes(Ah, -1, -2))).to(dev)
+    B, n = Acm.shape[0], Acm.shape[-1]
+    o_ref = torch.empty(B, dtype=torch.float64, device=dev)
+    o_eng = torch.empty(B, dtype=torch.float64, device=dev)
+    L = _lib.lib()
+    ms_ref = _ev_time(torch, stream, lambda: R.refgpu_pfaffian_f64(Acm.data_ptr(), B, n, o_ref.data_ptr(),
+                                                                   stream.cuda_stream), 3, 1)
+    ms_eng = _ev_time(torch, stream, lambda: L.pfb_pfaffian(_lib.F64, Acm.data_ptr(), B, n, _lib.COL_MAJOR,
+                                                           o_eng.data_ptr(), stream.cuda_stream), 10, 3)
+    torch.cuda.synchronize()
+    rel = float(torch.max(torch.abs(o_ref - o_eng) / torch.abs(o_eng)))
+    out["pfaffian_4096x32_f64"] = {"reference_ms": ms_ref, "engine_ms": ms_eng, "speedup": ms_ref / ms_eng,
+                                   "max_rel_diff": rel,
+                                   "how": "reference: pf_sm_calc once per matrix (4096 launches); "
+                                          "engine: pfb_pfaffian, one launch; same column-major buffer"}
+    for nn in (1024, 2048):
+        Al = O.config_large(nn, seed=1)[0]
+        X = torch.from_numpy(np.ascontiguousarray(Al.T)).to(dev)[None].contiguous()
+        tmp = torch.empty(nn * nn, dtype=torch.float64, device=dev)
+        l_ref = torch.empty(1, dtype=torch.float64, device=dev)
+        p_ref = torch.empty(1, dtype=torch.float64, device=dev)
+        ms_ref = _ev_time(torch, stream, lambda: R.refgpu_slog_f64(X.data_ptr(), 1, nn, l_ref.data_ptr(),
+                                                                   p_ref.data_ptr(), tmp.data_ptr(),
+                                                                   stream.cuda_stream), 2, 1)
+        res = {"reference_ms": ms_ref}
+        for mode in ("split", "fp64"):
+            ws = torch.empty(pf.slog_workspace_bytes(X.dtype, 1, nn, mode), dtype=torch.uint8, device=dev)
+            ms = _ev_time(torch, stream, lambda: pf.slog_pfaffian_raw(X, mode, layout=_lib.COL_MAJOR,
+                                                                      workspace=ws), 5, 2)
+            la, _ = pf.slog_pfaffian_raw(X, mode, layout=_lib.COL_MAJOR, workspace=ws)
+            res[f"engine_{mode}_ms"] = ms
+            res[f"speedup_{mode}"] = ms_ref / ms
+            res[f"log_diff_{mode}"] = float(torch.abs(la - l_ref)[0])
+        out[f"slog_pfaffian_{nn}_f64_batch1"] = res
+    out["note"] = ("the reference's large path copies one pivot to the host per pivot pair "
+                   "(src/slog_pfaffian_lg.cu:178), so its time is bound by those round trips")
+    return out
+
+
 def wl_small(torch, pf, _lib, O, dev, stream, steps, warmup, hbm_peak):
     """4096 independent 32x32 float64 matrices (seed 0): pfb_pfaffian, one launch."""
     L = _lib.lib()
@@ -375,8 +433,9 @@ def wl_illcond(torch, pf, _lib, O, dev, stream, steps, warmup):
     """64 float32 and 64 float64 matrices of order 2048, A = Q blockdiag(s_k J) Q^T,
     s_k log-spaced in [1e-6, 1] (seed 4): split-precision forward and VJP error
     against the exact log|Pf| and the FP64 oracle."""
-    Ah, exact_log, exact_sign = O.config_illcond()
+    Ah, exact_log, exact_sign, Qh = O.config_illcond(return_q=True)
     B, n = Ah.shape[0], Ah.shape[-1]
+    G_exact = O.illcond_half_inv_t(Qh[:2])       # (1/2) A^-T from the construction
     res = {"workload": "ill-conditioned: 64 float32 and 64 float64 matrices, 2n=2048, "
                        "A = Q blockdiag(s_k J) Q^T, Q Haar, s_k logspace(-6, 0), seed 4"}
     for name, npdt in (("float64", np.float64), ("float32", np.float32)):
@@ -394,9 +453,21 @@ def wl_illcond(torch, pf, _lib, O, dev, stream, steps, warmup):
              "max_log_rel_err_vs_fp64_oracle": float(np.max(np.abs(la[:sub] - wl) / np.abs(wl))),
              "oracle_matrices": sub}
         G = pf.slog_pfaffian_grad(A[:2], mode="split").cpu().numpy().astype(np.float64)
-        want = O.slog_pf_vjp(Ah[:2].astype(npdt).astype(np.float64))
-        r["vjp_max_rel_frobenius_err"] = float(np.max(
-            np.linalg.norm((G - want).reshape(2, -1), axis=1) / np.linalg.norm(want.reshape(2, -1), axis=1)))
+
+        def frob(X, Y):
+            return float(np.max(np.linalg.norm((X - Y).reshape(2, -1), axis=1) /
+                                np.linalg.norm(Y.reshape(2, -1), axis=1)))
+
+        if npdt == np.float64:
+            # the exact adjoint of the construction; bar cond * sqrt(n) * eps * 4
+            r["vjp_max_rel_frobenius_err_vs_exact"] = frob(G, G_exact)
+            r["vjp_bar"] = 1e6 * np.sqrt(n) * np.finfo(np.float64).eps * 4
+        else:
+            # the float32 matrices are the float64 ones rounded (cond 1e6), so the
+            # exact adjoint is out of reach; compared with NumPy's FP64 inverse of
+            # the rounded matrices, and the output is rounded to float32 once
+            r["vjp_max_rel_frobenius_err_vs_numpy_inverse"] = frob(
+                G, O.slog_pf_vjp(Ah[:2].astype(npdt).astype(np.float64)))
         res[name] = r
         del A, ws
         torch.cuda.empty_cache()
@@ -539,6 +610,31 @@ def main():
         if ck is not None:
             clocks = ck
         results1[m], _ = timed(m, 1, max(3, args.steps // 2))
+    tuned = {m: pf.slog_config(tdt, B, n, m) for m in modes}
+    tuned1 = {m: pf.slog_config(tdt, 1, n, m) for m in modes}
+
+    # each panel form at the headline batch, split and FP64 (a few calls each)
+    forms = {}
+    for m in modes:
+        for form in ("registers", "half_shared"):
+            if L.pfb_slog_max_concurrent_form(dtc, n, {"registers": 1, "half_shared": 2}[form]) <= 0:
+                continue
+            cfgx = {"panel": form}
+
+            def stepx(m=m, cfgx=cfgx):
+                pf.slog_pfaffian_raw(A, mode=m, workspace=ws[m], config=cfgx)
+
+            for _ in range(2):
+                stepx()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            kk = max(3, args.steps // 4)
+            for _ in range(kk):
+                stepx()
+            e1.record(stream)
+            barrier()
+            forms[f"{m}_{form}_ms"] = max_over_ranks(e0.elapsed_time(e1) / kk)
 
     # accuracy of the headline path against the FP64 oracle (rank 0)
     step(head)
@@ -623,13 +719,9 @@ def main():
 
     ms = results[head]
     value = world * B / (ms * 1e-3)
-    # kernel launches per call: the library runs a batch of three or more waves
-    # of the widest panel clusters (9 or more CTAs) as two ranges, each with
-    # its own sequence of launches
-    cpt = 1 if (nb == 64 or tdt == torch.complex128) else 2
-    widest = (n - nb + 256 * cpt - 1) // (256 * cpt)
-    mc = int(L.pfb_slog_max_concurrent(dtc, n))
-    ranges = 2 if (widest >= 9 and mc > 0 and B >= 3 * mc) else 1
+    # kernel launches per call: the library may run a batch as two ranges on two
+    # streams, each with its own sequence of launches
+    ranges = int(L.pfb_slog_stream_ranges(dtc, B, n, mc[head]))
     esz = A.element_size()
     hbm_peak = _hbm_peak()
     # trailing update, the kernel that carries the O(n^3) arithmetic: each of
@@ -673,6 +765,9 @@ def main():
                    "n": n, "batch": B, "mode": head, "panel_width": nb,
                    "l2": f"inputs {B * n * n * esz / 1e6:.0f} MB > 126 MB L2, re-read every step",
                    "parallelism": f"replicas x{world}"},
+        "tuned_config": tuned,
+        "tuned_config_batch1": tuned1,
+        "panel_forms_ms_per_step": forms,
         "modes_ms_per_step": results,
         "split_over_fp64": (results["fp64"] / results["split"]) if len(results) == 2 else None,
         "batch1_ms": results1,
@@ -700,6 +795,9 @@ def main():
         kw = dict(torch=torch, pf=pf, _lib=_lib, O=O, dev=dev, stream=stream, steps=args.steps,
                   warmup=args.warmup)
         line["peaks_measured_here"] = measure_peaks(torch, dev, stream)
+        t0 = time.perf_counter()
+        line["reference_gpu_baseline"] = reference_gpu_baseline(torch, pf, _lib, O, dev, stream)
+        line["reference_gpu_baseline"]["wall_s"] = time.perf_counter() - t0
         wls = {}
         for name, fn in (("small", wl_small), ("ragged", wl_ragged), ("grad", wl_grad),
                          ("illcond", wl_illcond)):

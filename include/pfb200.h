@@ -212,6 +212,21 @@ int pfb_slog_max_concurrent_form(int dtype, int n, int panel);
 int pfb_slog_stream_ranges(int dtype, int64_t batch, int n, int mode);
 
 /*
+ * pfb_slog_pfaffian on a batch given as matrix pointers: A_ptrs is a DEVICE
+ * array of `batch` pointers, each to one contiguous n x n matrix of `dtype` in
+ * `layout` (the matrices need not be adjacent or in order).  n must be even and
+ * above 32 (PFB_ERR_SIZE otherwise).  Results, workspace
+ * (pfb_slog_workspace_bytes) and configuration are those of pfb_slog_pfaffian.
+ * It serves ragged batches whose orders exceed PFB_RAGGED_MAX_N: one call per
+ * order on the matrices of that order, wherever they lie.  No reference
+ * counterpart (the reference's caller loops over matrices,
+ * pfcuda/cuda_api.py:57-76).
+ */
+int pfb_slog_pfaffian_ptrs(int dtype, const void *const *A_ptrs, int64_t batch, int n, int layout,
+                           int mode, double *log_out, void *sign_out, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
+/*
  * (log|Pf|, sign) of a ragged batch in one launch: `count` matrices of even (or
  * odd) orders n[i] <= max_n <= PFB_RAGGED_MAX_N, each float32 or float64
  * (dtype[i]), each contiguous at A[i] in `layout`.  A, n and dtype are DEVICE

@@ -128,6 +128,17 @@ def slog_pf(A, with_pivots=False):
     return la, sign
 
 
+def slog_pf_list(mats):
+    """slog_pf of each matrix of a list of square matrices of any orders:
+    (log|Pf|, sign) as two float64 arrays (real input)."""
+    la = np.empty(len(mats))
+    sg = np.empty(len(mats))
+    for i, M in enumerate(mats):
+        l_, s_ = slog_pf(np.asarray(M)[None])
+        la[i], sg[i] = l_[0], s_[0]
+    return la, sg
+
+
 def pf_product(A, as_shipped=False):
     """Plain product Pf per matrix (the value the reference returns), in FP64 / C128.
 

@@ -36,6 +36,7 @@ SIGNATURES = {
     "pfb_slog_max_concurrent_form": (_int, [_int, _int, _int]),
     "pfb_slog_config_for": (_int, [_int, _i64, _int, _int, _vp]),
     "pfb_slog_pfaffian_ex": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),
+    "pfb_slog_pfaffian_ptrs": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp, _sz, _vp]),
     "pfb_slog_pfaffian_ragged": (_int, [_vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp, _sz, _vp]),
     "pfb_slog_ragged_workspace_bytes": (_sz, [_i64, _int]),
     "pfb_slog_pfaffian_noalloc": (_int, [_int, _vp, _i64, _int, _int, _int, _vp, _vp, _vp]),

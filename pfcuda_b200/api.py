@@ -223,17 +223,24 @@ def upload_upper_bytes(dtype: torch.dtype, batch: int, n: int) -> int:
 # ------------------------------------------------------------- ragged batches
 
 class RaggedPlan:
-    """A ragged batch prepared once and run many times (one launch per run).
+    """A ragged batch prepared once and run many times.
 
     ``mats`` is a list of square CUDA tensors (float32 or float64, row-major
-    unless ``layout`` says otherwise) of even or odd orders up to 544.  The
-    device arrays of pointers, orders and dtypes and the workspace are built here;
-    ``run()`` enqueues the sort and the persistent factorisation kernel on the
-    current stream and returns (log|Pf|, sign) as float64 tensors.  ``run()``
-    allocates nothing, so it may be captured in a torch.cuda.CUDAGraph.
+    unless ``layout`` says otherwise) of any orders.  Orders up to
+    PFB_RAGGED_MAX_N (544) share one persistent launch (pfb_slog_pfaffian_ragged:
+    a device-side sort, largest first, and an atomic work queue, every matrix
+    factored in FP64); larger orders -- the large bin -- go to the blocked
+    cluster-panel path, one pfb_slog_pfaffian_ptrs call per (order, dtype) on
+    the matrices where they lie, in ``mode`` ("auto": split-precision update).
+    The device arrays of pointers, orders and dtypes, the workspaces and the
+    index maps are built here; ``run()`` enqueues everything on the current
+    stream and returns (log|Pf|, sign) as float64 tensors in the input order.
+    ``run()`` allocates nothing, so it may be captured in a torch.cuda.CUDAGraph.
     """
 
-    def __init__(self, mats, layout: int = _lib.ROW_MAJOR):
+    RAGGED_MAX_N = 544
+
+    def __init__(self, mats, layout: int = _lib.ROW_MAJOR, mode: str = "auto"):
         if not mats:
             raise ValueError("empty batch")
         dev = mats[0].device
@@ -246,30 +253,104 @@ class RaggedPlan:
                 raise ValueError("all matrices must be CUDA tensors on one device")
         self.mats = [M.contiguous() for M in mats]
         self.count = len(self.mats)
-        self.max_n = max(M.shape[0] for M in self.mats)
-        if self.max_n > 544:
-            raise ValueError("ragged batches take orders up to 544")
         self.layout = layout
-        self.ptrs = torch.tensor([M.data_ptr() for M in self.mats], dtype=torch.int64, device=dev)
-        self.ns = torch.tensor([M.shape[0] for M in self.mats], dtype=torch.int32, device=dev)
-        self.dts = torch.tensor([_DT[M.dtype] for M in self.mats], dtype=torch.int32, device=dev)
-        wsb = int(_lib.lib().pfb_slog_ragged_workspace_bytes(self.count, self.max_n))
-        self.ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        self.mode = resolve_mode(mode, torch.float64)
+        orders = [M.shape[0] for M in self.mats]
+        self.max_n = max(orders)
+        small = [i for i, m in enumerate(orders) if m <= self.RAGGED_MAX_N]
+        odd_large = [i for i, m in enumerate(orders) if m > self.RAGGED_MAX_N and m & 1]
+        groups = {}
+        for i, m in enumerate(orders):
+            if m > self.RAGGED_MAX_N and not m & 1:
+                groups.setdefault((m, self.mats[i].dtype), []).append(i)
+        L = _lib.lib()
         self.log = torch.empty(self.count, dtype=torch.float64, device=dev)
         self.sign = torch.empty(self.count, dtype=torch.float64, device=dev)
+        # odd orders above the ragged bin: Pf = 0, set once here, never rewritten
+        if odd_large:
+            oi = torch.tensor(odd_large, dtype=torch.int64, device=dev)
+            self.log.index_fill_(0, oi, -float("inf"))
+            self.sign.index_fill_(0, oi, 0.0)
+        self._direct = len(small) == self.count
+        self._small = None
+        if small:
+            sm_mats = [self.mats[i] for i in small]
+            ns = max(orders[i] for i in small)
+            self._small_n = ns
+            self._ptrs = torch.tensor([M.data_ptr() for M in sm_mats], dtype=torch.int64, device=dev)
+            self._ns = torch.tensor([M.shape[0] for M in sm_mats], dtype=torch.int32, device=dev)
+            self._dts = torch.tensor([_DT[M.dtype] for M in sm_mats], dtype=torch.int32, device=dev)
+            wsb = int(L.pfb_slog_ragged_workspace_bytes(len(sm_mats), ns))
+            self._ws_small = torch.empty(wsb, dtype=torch.uint8, device=dev)
+            if self._direct:
+                self._log_s, self._sign_s = self.log, self.sign
+            else:
+                self._log_s = torch.empty(len(small), dtype=torch.float64, device=dev)
+                self._sign_s = torch.empty(len(small), dtype=torch.float64, device=dev)
+                self._idx_s = torch.tensor(small, dtype=torch.int64, device=dev)
+            self._small = len(small)
+        # the large bin: one pointer-array call per (order, dtype); the calls run
+        # one after another on the stream, so they share one workspace
+        self._groups = []
+        wmax = 0
+        for (m, dt), idx in sorted(groups.items(), key=lambda kv: -kv[0][0]):
+            ptrs = torch.tensor([self.mats[i].data_ptr() for i in idx], dtype=torch.int64, device=dev)
+            lg = torch.empty(len(idx), dtype=torch.float64, device=dev)
+            sg = torch.empty(len(idx), dtype=dt, device=dev)
+            # float32 signs are widened through a preallocated buffer
+            sgd = sg if dt == torch.float64 else torch.empty(len(idx), dtype=torch.float64, device=dev)
+            it = torch.tensor(idx, dtype=torch.int64, device=dev)
+            wsb = int(L.pfb_slog_workspace_bytes(_DT[dt], len(idx), m, _MODES[self.mode]))
+            if wsb == 0:
+                raise ValueError(f"order {m} is beyond the large path")
+            wmax = max(wmax, wsb)
+            self._groups.append((m, dt, ptrs, lg, sg, sgd, it, wsb))
+        self._ws_large = torch.empty(max(wmax, 1), dtype=torch.uint8, device=dev) if self._groups else None
+
+    @property
+    def launches(self) -> int:
+        """Kernel launches of one run() (the ragged pair, each large call's
+        sequence, and the scatters)."""
+        L = _lib.lib()
+        k = 2 if self._small else 0
+        if self._small and not self._direct:
+            k += 2
+        for (m, dt, ptrs, lg, sg, sgd, it, wsb) in self._groups:
+            nb = int(L.pfb_slog_panel_width(_DT[dt], m))
+            npan = (m - 1 + nb - 1) // nb
+            per = 2 + npan + (npan - 1) * (2 if self.mode == "split" else 1)
+            k += per * int(L.pfb_slog_stream_ranges(_DT[dt], ptrs.numel(), m, _MODES[self.mode]))
+            k += 2 + (0 if sgd is sg else 1)
+        return k
 
     def run(self):
-        st = _lib.lib().pfb_slog_pfaffian_ragged(
-            self.ptrs.data_ptr(), self.ns.data_ptr(), self.dts.data_ptr(), self.count, self.max_n,
-            self.layout, self.log.data_ptr(), self.sign.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
-            _stream(self.log))
-        _lib.check(st, "pfb_slog_pfaffian_ragged")
+        L = _lib.lib()
+        stream = _stream(self.log)
+        if self._small:
+            st = L.pfb_slog_pfaffian_ragged(
+                self._ptrs.data_ptr(), self._ns.data_ptr(), self._dts.data_ptr(), self._small, self._small_n,
+                self.layout, self._log_s.data_ptr(), self._sign_s.data_ptr(), self._ws_small.data_ptr(),
+                self._ws_small.numel(), stream)
+            _lib.check(st, "pfb_slog_pfaffian_ragged")
+            if not self._direct:
+                self.log.index_copy_(0, self._idx_s, self._log_s)
+                self.sign.index_copy_(0, self._idx_s, self._sign_s)
+        for (m, dt, ptrs, lg, sg, sgd, it, wsb) in self._groups:
+            st = L.pfb_slog_pfaffian_ptrs(_DT[dt], ptrs.data_ptr(), ptrs.numel(), m, self.layout,
+                                          _MODES[self.mode], lg.data_ptr(), sg.data_ptr(),
+                                          self._ws_large.data_ptr(), wsb, stream)
+            _lib.check(st, "pfb_slog_pfaffian_ptrs")
+            if sgd is not sg:
+                sgd.copy_(sg)
+            self.log.index_copy_(0, it, lg)
+            self.sign.index_copy_(0, it, sgd)
         return self.log, self.sign
 
 
-def slog_pfaffian_ragged(mats, layout: int = _lib.ROW_MAJOR):
-    """(log|Pf|, sign) for a list of matrices of different orders, in one launch."""
-    plan = RaggedPlan(mats, layout)
+def slog_pfaffian_ragged(mats, layout: int = _lib.ROW_MAJOR, mode: str = "auto"):
+    """(log|Pf|, sign) for a list of matrices of different orders: orders up to
+    544 in one launch, larger ones through the blocked path (RaggedPlan)."""
+    plan = RaggedPlan(mats, layout, mode)
     la, sg = plan.run()
     return la.clone(), sg.clone()
 

@@ -139,6 +139,24 @@ int pfb_slog_pfaffian_ex(int dtype, const void *A, int64_t batch, int n, int lay
     return rc;
 }
 
+int pfb_slog_pfaffian_ptrs(int dtype, const void *const *A_ptrs, int64_t batch, int n, int layout, int mode,
+                           double *log_out, void *sign_out, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!valid_dtype(dtype) || !valid_layout(layout) || batch < 0 || n < 0) return PFB_ERR_INVALID;
+    if ((mode & 0xff) != PFB_MODE_FP64 && (mode & 0xff) != PFB_MODE_SPLIT) return PFB_ERR_INVALID;
+    if ((mode & ~0xfff) != 0 || ((mode >> 8) & 0xf) > 7) return PFB_ERR_INVALID;
+    if (n <= 32 || (n & 1)) return PFB_ERR_SIZE;
+    if (batch == 0) return PFB_OK;
+    if (!A_ptrs || !log_out || !sign_out) return PFB_ERR_INVALID;
+    const size_t need = pfb::large_workspace_bytes(dtype, batch, n, mode);
+    if (need == 0) return PFB_ERR_SIZE;
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
+    const int rc = pfb::launch_large(dtype, nullptr, batch, n, layout, mode, log_out, sign_out, workspace,
+                                     workspace_bytes, (cudaStream_t)stream, nullptr, nullptr, A_ptrs);
+    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    return rc;
+}
+
 size_t pfb_slog_grad_workspace_bytes(int dtype, int64_t batch, int n, int mode)
 {
     if (!valid_dtype(dtype) || batch < 0 || n < 2 || (n & 1)) return 0;

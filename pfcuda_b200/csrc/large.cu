@@ -115,16 +115,18 @@ size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode)
 // W <- A widened, the upper triangle only (diagonal included): nothing reads
 // below the diagonal of W.  One warp per row at a time, the row's columns
 // r .. n-1 in coalesced runs of 32.
+// The matrices come either contiguous from A or, when Ap is set, one pointer
+// per matrix (Ap[b], a device array).
 template <typename S, typename T>
-__global__ void copy_in_kernel(const S *__restrict__ A, T *__restrict__ W, int64_t batch, int n,
-                               MatState *st)
+__global__ void copy_in_kernel(const S *__restrict__ A, const S *const *__restrict__ Ap, T *__restrict__ W,
+                               int64_t batch, int n, MatState *st)
 {
     const int lane = threadIdx.x & 31;
     const int64_t rows = batch * n;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t R = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; R < rows; R += nwarps) {
         const int r = (int)(R % n);
-        const S *src = A + R * n;
+        const S *src = Ap ? Ap[R / n] + (int64_t)r * n : A + R * n;
         T *dst = W + R * n;
         for (int c = r + lane; c < n; c += 32) dst[c] = conv<T>(src[c]);
     }
@@ -356,8 +358,8 @@ template <typename T, int NB, int CPT>
 // Matrices [b0, b0 + B) of a call on `batch` matrices, on stream s: the
 // workspace is laid out for the whole call and this range uses its slices of
 // it (A, log_out and sign_out are already offset to matrix b0).
-static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_t B, int n, int layout,
-                     int mode, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s,
+static int run_large(const void *A, const void *const *Ap, int dtype, int64_t batch, int64_t b0, int64_t B, int n,
+                     int layout, int mode, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s,
                      const pfb_slog_timing *tm, const pfb_slog_config &cf)
 {
     const LargeLayout L = large_layout(dtype, batch, n, mode);
@@ -374,16 +376,16 @@ static int run_large(const void *A, int dtype, int64_t batch, int64_t b0, int64_
         if (blocks < 1) blocks = 1;
         switch (dtype) {
         case PFB_F32:
-            copy_in_kernel<float, double><<<(unsigned)blocks, 256, 0, s>>>((const float *)A, (double *)W, B, n, st);
+            copy_in_kernel<float, double><<<(unsigned)blocks, 256, 0, s>>>((const float *)A, (const float *const *)Ap, (double *)W, B, n, st);
             break;
         case PFB_F64:
-            copy_in_kernel<double, double><<<(unsigned)blocks, 256, 0, s>>>((const double *)A, (double *)W, B, n, st);
+            copy_in_kernel<double, double><<<(unsigned)blocks, 256, 0, s>>>((const double *)A, (const double *const *)Ap, (double *)W, B, n, st);
             break;
         case PFB_C64:
-            copy_in_kernel<c64, c128><<<(unsigned)blocks, 256, 0, s>>>((const c64 *)A, (c128 *)W, B, n, st);
+            copy_in_kernel<c64, c128><<<(unsigned)blocks, 256, 0, s>>>((const c64 *)A, (const c64 *const *)Ap, (c128 *)W, B, n, st);
             break;
         default:
-            copy_in_kernel<c128, c128><<<(unsigned)blocks, 256, 0, s>>>((const c128 *)A, (c128 *)W, B, n, st);
+            copy_in_kernel<c128, c128><<<(unsigned)blocks, 256, 0, s>>>((const c128 *)A, (const c128 *const *)Ap, (c128 *)W, B, n, st);
             break;
         }
         if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
@@ -543,23 +545,25 @@ static bool hs_available(int dtype, int n)
     return large_cfg(dtype, n, &nb, &cpt) && cpt == 1;
 }
 
-static int run_large_range(int dtype, const void *A, int64_t batch, int64_t b0, int64_t B, int n, int layout,
-                           int mode, double *log_out, void *sign_out, unsigned char *ws, cudaStream_t s,
-                           const pfb_slog_timing *timing, const pfb_slog_config &cf)
+static int run_large_range(int dtype, const void *A, const void *const *Ap, int64_t batch, int64_t b0, int64_t B,
+                           int n, int layout, int mode, double *log_out, void *sign_out, unsigned char *ws,
+                           cudaStream_t s, const pfb_slog_timing *timing, const pfb_slog_config &cf)
 {
     int nb = 0, cpt = 0;
     large_cfg(dtype, n, &nb, &cpt);
     const size_t in_es = dtype == PFB_F32 ? 4 : (dtype == PFB_C128 ? 16 : 8);
     const size_t sign_es = in_es;
-    const void *a = static_cast<const char *>(A) + (size_t)b0 * (size_t)n * (size_t)n * in_es;
+    const void *a = Ap ? nullptr : static_cast<const char *>(A) + (size_t)b0 * (size_t)n * (size_t)n * in_es;
+    const void *const *ap = Ap ? Ap + b0 : nullptr;
     double *lo = log_out + b0;
     void *so = static_cast<char *>(sign_out) + (size_t)b0 * sign_es;
     const bool cplx = dtype == PFB_C64 || dtype == PFB_C128;
     if (!cplx) {
-        if (nb == 64) return run_large<double, 64, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
-        return run_large<double, 32, 2>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
+        if (nb == 64)
+            return run_large<double, 64, 1>(a, ap, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
+        return run_large<double, 32, 2>(a, ap, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
     }
-    return run_large<c128, 32, 1>(a, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
+    return run_large<c128, 32, 1>(a, ap, dtype, batch, b0, B, n, layout, mode, lo, so, ws, s, timing, cf);
 }
 
 // The second stream of this host thread's calls on device `dev`: one per thread
@@ -648,7 +652,8 @@ int64_t large_second_range(int dtype, int64_t batch, int n, const pfb_slog_confi
 
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
-                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *over)
+                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *over,
+                 const void *const *A_ptrs)
 {
     int nb = 0, cpt = 0;
     if (!large_cfg(dtype, n, &nb, &cpt)) return PFB_ERR_SIZE;
@@ -663,7 +668,8 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
     if (mc > 0 && cudaGetDevice(&dev) == cudaSuccess) s2 = aux_stream(dev);
     if (s2 && !aux_usable(stream, s2)) s2 = nullptr;
     if (!s2)
-        return run_large_range(dtype, A, batch, 0, batch, n, layout, mode, log_out, sign_out, ws, stream, timing, cf);
+        return run_large_range(dtype, A, A_ptrs, batch, 0, batch, n, layout, mode, log_out, sign_out, ws, stream,
+                               timing, cf);
 
     const int64_t B2 = mc, B1 = batch - B2;
     cudaEvent_t fork, join;
@@ -676,10 +682,11 @@ int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int
     if (cudaEventRecord(fork, stream) != cudaSuccess || cudaStreamWaitEvent(s2, fork, 0) != cudaSuccess)
         rc = PFB_ERR_CUDA;
     if (rc == PFB_OK)
-        rc = run_large_range(dtype, A, batch, 0, B1, n, layout, mode, log_out, sign_out, ws, stream, nullptr, cf);
+        rc = run_large_range(dtype, A, A_ptrs, batch, 0, B1, n, layout, mode, log_out, sign_out, ws, stream, nullptr,
+                             cf);
     // the second range always runs (or at least joins), so the fork is always closed
-    const int rc2 = rc == PFB_OK ? run_large_range(dtype, A, batch, B1, B2, n, layout, mode, log_out, sign_out, ws,
-                                                   s2, nullptr, cf)
+    const int rc2 = rc == PFB_OK ? run_large_range(dtype, A, A_ptrs, batch, B1, B2, n, layout, mode, log_out,
+                                                   sign_out, ws, s2, nullptr, cf)
                                  : PFB_OK;
     if (cudaEventRecord(join, s2) != cudaSuccess || cudaStreamWaitEvent(stream, join, 0) != cudaSuccess)
         rc = PFB_ERR_CUDA;

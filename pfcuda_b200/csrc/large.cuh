@@ -22,7 +22,8 @@ size_t large_workspace_bytes(int dtype, int64_t batch, int n, int mode);
 
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
                  double *log_out, void *sign_out, void *workspace, size_t workspace_bytes,
-                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *config = nullptr);
+                 cudaStream_t stream, const pfb_slog_timing *timing, const pfb_slog_config *config = nullptr,
+                 const void *const *A_ptrs = nullptr);
 bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_config *over, pfb_slog_config *out);
 
 int large_panel_width(int dtype, int n);

@@ -11,12 +11,17 @@ module holds the host-side logic:
 * ``slog_pfaffian_sharded`` -- each rank factors its slice of a uniform batch
   and, if asked, the per-matrix results are gathered on every rank with one
   all_gather of (log|Pf|, sign) -- 16 or 24 bytes per matrix, the only
-  collective, after all compute.
+  collective, after all compute;
+* ``pfaffian_sharded`` -- the same for the small path (2n <= 32);
+* ``slog_pfaffian_ragged_sharded`` -- a ragged batch split by ``shard_ragged``,
+  each rank running its matrices through one RaggedPlan, the results gathered
+  back into the input order;
+* ``slog_pfaffian_grad_sharded`` -- the adjoint ct * (1/2) A^-T of each rank's
+  slice, the gradients (n^2 values per matrix) gathered if asked.
 
 Every rank takes the same collective steps in the same order.  ``compute``
-is the per-rank function (log, sign) = compute(A_slice); it defaults to the
-engine's ``slog_pfaffian_raw`` and is replaceable so that the host logic can be
-exercised on CPU process groups (gloo).
+is the per-rank function; it defaults to the engine's call and is replaceable
+so that the host logic can be exercised on CPU process groups (gloo).
 """
 from __future__ import annotations
 
@@ -58,6 +63,48 @@ def _default_compute(A):
     return slog_pfaffian_raw(A.contiguous())
 
 
+def _group_info(group):
+    import torch.distributed as dist
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        return None
+    return dist.get_world_size(group), dist.get_rank(group)
+
+
+def _gather_padded(x: torch.Tensor, counts, group):
+    """Concatenation over ranks of each rank's x (counts[r] rows on rank r), in
+    rank order, through one all_gather of row blocks padded to the largest
+    count.  A complex tensor travels as its (re, im) pairs."""
+    import torch.distributed as dist
+    world = len(counts)
+    width = max(counts) if counts else 0
+    cplx = x.is_complex()
+    xr = torch.view_as_real(x) if cplx else x
+    pad = torch.zeros((width,) + tuple(xr.shape[1:]), dtype=xr.dtype, device=xr.device)
+    pad[: xr.shape[0]] = xr
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    out = torch.cat([parts[r][: counts[r]] for r in range(world)])
+    return torch.view_as_complex(out.contiguous()) if cplx else out
+
+
+def _sharded_uniform(A, group, compute, gather):
+    """compute(A[lo:hi]) on each rank's contiguous slice; each output (a tensor
+    or a tuple of tensors with one leading row per matrix) gathered if asked."""
+    info = _group_info(group)
+    if info is None:
+        return compute(A)
+    world, rank = info
+    B = A.shape[0]
+    lo, hi = shard_range(B, world, rank)
+    out = compute(A[lo:hi])
+    if not gather:
+        return out
+    counts = [shard_range(B, world, r)[1] - shard_range(B, world, r)[0] for r in range(world)]
+    if isinstance(out, tuple):
+        return tuple(_gather_padded(o, counts, group) for o in out)
+    return _gather_padded(out, counts, group)
+
+
 def slog_pfaffian_sharded(A: torch.Tensor, group=None, compute=None, gather: bool = True):
     """(log|Pf|, sign) of a (B, n, n) batch, each rank factoring its shard.
 
@@ -66,34 +113,76 @@ def slog_pfaffian_sharded(A: torch.Tensor, group=None, compute=None, gather: boo
     the rank's own slice.  Without an initialised process group this is the
     single-GPU call.
     """
-    import torch.distributed as dist
+    return _sharded_uniform(A, group, compute or _default_compute, gather)
 
-    compute = compute or _default_compute
-    if group is None and not (dist.is_available() and dist.is_initialized()):
-        return compute(A)
-    world = dist.get_world_size(group)
-    rank = dist.get_rank(group)
+
+def pfaffian_sharded(A: torch.Tensor, group=None, compute=None, gather: bool = True):
+    """Pf of a (B, n, n) batch with 2n <= 32, each rank computing its shard
+    (one pfb_pfaffian launch per rank); gathered as slog_pfaffian_sharded."""
+    if compute is None:
+        from .api import pfaffian_raw
+
+        def compute(X):
+            return pfaffian_raw(X.contiguous())
+    return _sharded_uniform(A, group, compute, gather)
+
+
+def slog_pfaffian_grad_sharded(A: torch.Tensor, ct: torch.Tensor | None = None, group=None, compute=None,
+                               gather: bool = True, mode: str = "fp64"):
+    """ct * (1/2) A^-T of a (B, n, n) batch, each rank differentiating its shard
+    (one pfb_slog_pfaffian_grad call per rank).  ``ct``: one real cotangent per
+    matrix of the full batch, or None.  With ``gather`` every rank gets the full
+    (B, n, n) gradient (one all_gather of n^2 values per matrix), else its own
+    slice."""
+    info = _group_info(group)
     B = A.shape[0]
+    if compute is None:
+        from .grad import slog_pfaffian_grad
+
+        def compute(X, c):
+            return slog_pfaffian_grad(X.contiguous(), ct=c, mode=mode)
+    if info is None:
+        return compute(A, ct)
+    world, rank = info
     lo, hi = shard_range(B, world, rank)
-    la, sg = compute(A[lo:hi])
+    return _sharded_uniform(A, group, lambda X: compute(X, None if ct is None else ct[lo:hi]), gather)
+
+
+def slog_pfaffian_ragged_sharded(mats, group=None, compute=None, gather: bool = True):
+    """(log|Pf|, sign) of a ragged batch split across ranks by shard_ragged.
+
+    Every rank passes the same list; of the other ranks' matrices only the
+    order (the shape) is read, so they may be placeholders of the right shape
+    (for instance meta tensors).  ``compute`` maps
+    the rank's list of matrices to (log, sign) float64 tensors (default:
+    slog_pfaffian_ragged).  With ``gather`` the results come back on every rank
+    in the input order (one all_gather of 16 bytes per matrix); else the
+    rank's own results with their input indices: (log, sign, indices).
+    """
+    orders = [int(M.shape[-1]) for M in mats]
+    if compute is None:
+        from .api import slog_pfaffian_ragged as compute
+    info = _group_info(group)
+    if info is None:
+        return compute(list(mats))
+    world, rank = info
+    plan = shard_ragged(orders, world)
+    mine = plan[rank]
+    if mine:
+        la, sg = compute([mats[i] for i in mine])
+    else:
+        dev = mats[0].device if len(mats) else torch.device("cpu")
+        la = torch.empty(0, dtype=torch.float64, device=dev)
+        sg = torch.empty(0, dtype=torch.float64, device=dev)
+    idx = torch.tensor(mine, dtype=torch.int64, device=la.device)
     if not gather:
-        return la, sg
-    # pad every shard to the largest one so all_gather sees equal sizes; a
-    # complex sign travels as its (re, im) pairs
-    width = -(-B // world)
-    cplx = sg.is_complex()
-    sg_r = torch.view_as_real(sg) if cplx else sg
-    pad_l = torch.full((width,), float("nan"), dtype=la.dtype, device=la.device)
-    pad_s = torch.zeros((width,) + tuple(sg_r.shape[1:]), dtype=sg_r.dtype, device=sg.device)
-    pad_l[: hi - lo] = la
-    pad_s[: hi - lo] = sg_r
-    all_l = [torch.empty_like(pad_l) for _ in range(world)]
-    all_s = [torch.empty_like(pad_s) for _ in range(world)]
-    dist.all_gather(all_l, pad_l, group=group)
-    dist.all_gather(all_s, pad_s, group=group)
-    sizes = [shard_range(B, world, r)[1] - shard_range(B, world, r)[0] for r in range(world)]
-    out_l = torch.cat([all_l[r][: sizes[r]] for r in range(world)])
-    out_s = torch.cat([all_s[r][: sizes[r]] for r in range(world)])
-    if cplx:
-        out_s = torch.view_as_complex(out_s.contiguous())
+        return la, sg, idx
+    counts = [len(p) for p in plan]
+    all_l = _gather_padded(la, counts, group)
+    all_s = _gather_padded(sg, counts, group)
+    order = torch.tensor([i for p in plan for i in p], dtype=torch.int64, device=la.device)
+    out_l = torch.empty(len(orders), dtype=all_l.dtype, device=la.device)
+    out_s = torch.empty(len(orders), dtype=all_s.dtype, device=la.device)
+    out_l[order] = all_l
+    out_s[order] = all_s
     return out_l, out_s

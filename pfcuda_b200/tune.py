@@ -1,0 +1,181 @@
+"""Autotuner of the large path: writes pfcuda_b200/tune_table.json.
+
+    python -m pfcuda_b200.tune [--quick] [--out PATH]
+
+For each dtype class (real: float64 working precision, complex: complex128),
+mode (split, fp64), order bin and batch bin it times every configuration the
+library offers (pfb_slog_config: panel form, stream ranges, split digits) on
+seeded synthetic matrices and keeps the fastest one that meets the accuracy
+bar.  The build (pfcuda_b200/build.py) compiles the table into
+csrc/tune_table.h; pfb_slog_pfaffian then uses it whenever the caller gives no
+configuration of its own.
+
+Knobs:
+  panel   registers (one CTA per SM) | half_shared (two CTAs per SM; orders up
+          to 4160 real / 2080 complex)
+  ranges  1 | 2 (a batch of three or more waves of wide panel clusters split
+          over two streams)
+  slices  int8 digits per operand of the split update: 7 always qualifies; 6
+          and 5 are kept only where the log error stays within
+          --accuracy-margin x 1e-10 relative both on random matrices (against
+          the FP64 path) and on the ill-conditioned construction
+          A = Q blockdiag(s_k J) Q^T, s_k in [1e-6, 1] (against its exact value).
+
+Timing: CUDA events on the launching stream around `reps` calls after two
+warm-up calls; inputs of the larger orders exceed the 126 MB L2, smaller ones
+are re-read from L2 as a serving loop would.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# order bins: (n_min, n_max, representative order); complex stops at 2080
+REAL_BINS = [(34, 544, 512), (546, 1056, 1024), (1058, 2080, 2048), (2082, 4160, 4096), (4162, 8224, 6144)]
+CPLX_BINS = [(34, 544, 512), (546, 1056, 1024), (1058, 2080, 2048)]
+
+
+def skew(rng, B, n, cplx):
+    G = rng.normal(scale=1 / np.sqrt(n), size=(B, n, n))
+    if cplx:
+        G = G + 1j * rng.normal(scale=1 / np.sqrt(n), size=(B, n, n))
+    return (G - np.swapaxes(G, -1, -2)) / 2
+
+
+def illcond(rng, n):
+    """One matrix Q blockdiag(s_k J) Q^T with Q Haar and its exact log|Pf|."""
+    s = np.logspace(-6, 0, n // 2)
+    Q, R = np.linalg.qr(rng.normal(size=(n, n)))
+    Q = Q * np.sign(np.diag(R))
+    idx = np.arange(0, n, 2)
+    M = (Q[:, idx] * s) @ Q[:, idx + 1].T
+    A = M - M.T
+    return A[None], float(np.sum(np.log(s)))
+
+
+def time_call(pf, X, mode, cfg, ws, reps):
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        pf.slog_pfaffian_raw(X, mode=mode, workspace=ws, config=cfg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        pf.slog_pfaffian_raw(X, mode=mode, workspace=ws, config=cfg)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def slices_ok(pf, n, cplx, slices, margin, cache):
+    """Whether `slices` digits keep the split path within margin * 1e-10 of
+    the reference values at order n (random: the FP64 path; ill-conditioned,
+    real only: the exact value)."""
+    key = (n, cplx, slices)
+    if key in cache:
+        return cache[key]
+    rng = np.random.default_rng(11 + n)
+    A = torch.from_numpy(skew(rng, 2, n, cplx)).cuda()
+    cfg = {"slices": slices, "ranges": 1}
+    l_s, _ = pf.slog_pfaffian_raw(A, mode="split", config=cfg)
+    l_f, _ = pf.slog_pfaffian_raw(A, mode="fp64")
+    err = float(torch.max(torch.abs(l_s - l_f) / torch.abs(l_f)))
+    if not cplx:
+        B, exact = illcond(rng, n)
+        l_i, _ = pf.slog_pfaffian_raw(torch.from_numpy(B).cuda(), mode="split", config=cfg)
+        err = max(err, abs(float(l_i[0]) - exact) / abs(exact))
+    ok = err <= margin * 1e-10
+    cache[key] = ok
+    print(f"  accuracy n={n} {'c128' if cplx else 'f64'} slices={slices}: rel err {err:.2e} "
+          f"{'ok' if ok else 'rejected'}", file=sys.stderr)
+    return ok
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(HERE, "tune_table.json"))
+    ap.add_argument("--quick", action="store_true", help="fewer orders and repetitions")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--accuracy-margin", type=float, default=0.1,
+                    help="fraction of the 1e-10 bar a reduced digit count may use")
+    ap.add_argument("--max-input-gb", type=float, default=3.0)
+    args = ap.parse_args()
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    import pfcuda_b200 as pf
+    from pfcuda_b200 import _lib
+
+    L = _lib.lib()
+    dev = torch.cuda.get_device_properties(0)
+    entries, log = [], []
+    acc_cache = {}
+    t_start = time.time()
+    for cplx in (False, True):
+        bins = CPLX_BINS if cplx else REAL_BINS
+        if args.quick:
+            bins = [b for b in bins if b[2] in (1024, 4096)]
+        dtc = _lib.C128 if cplx else _lib.F64
+        tdt = torch.complex128 if cplx else torch.float64
+        esz = 16 if cplx else 8
+        for (n_min, n_max, n) in bins:
+            m1 = L.pfb_slog_max_concurrent_form(dtc, n, _lib.PANEL_REGISTERS)
+            m2 = L.pfb_slog_max_concurrent_form(dtc, n, _lib.PANEL_HALF_SHARED)
+            if m1 <= 0:
+                continue
+            cap = max(1, int(args.max_input_gb * 1e9 // (n * n * esz)))
+            # batch bins: one matrix; one wave of the register form; many waves
+            bb = [(1, 1, 1), (2, 3 * m1 - 1, min(m1, cap)), (3 * m1, 1 << 40, min(4 * m1, cap))]
+            rng = np.random.default_rng(1)
+            Xall = torch.from_numpy(skew(rng, max(b[2] for b in bb), n, cplx)).cuda()
+            for (b_min, b_max, B) in bb:
+                X = Xall[:B].contiguous()
+                for mode in ("split", "fp64"):
+                    ws = torch.empty(pf.slog_workspace_bytes(tdt, B, n, mode), dtype=torch.uint8, device="cuda")
+                    panels = ["registers"] + (["half_shared"] if m2 > 0 else [])
+                    slices = [7, 6, 5] if mode == "split" else [7]
+                    best = None
+                    for panel in panels:
+                        for ranges in (1, 2):
+                            for sl in slices:
+                                if sl < 7 and not slices_ok(pf, n, cplx, sl, args.accuracy_margin, acc_cache):
+                                    continue
+                                cfg = {"panel": panel, "ranges": ranges, "slices": sl}
+                                ms = time_call(pf, X, mode, cfg, ws, args.reps)
+                                log.append({"dtype": "complex" if cplx else "real", "mode": mode, "n": n,
+                                            "batch": B, **cfg, "ms": ms})
+                                if best is None or ms < best[0]:
+                                    best = (ms, cfg)
+                    ms, cfg = best
+                    print(f"{'c128' if cplx else 'f64'} {mode} n={n} batch={B}: {cfg} {ms:.3f} ms "
+                          f"({B / ms * 1e3:.1f} matrices/s)", file=sys.stderr)
+                    entries.append({"dtype": "complex" if cplx else "real", "mode": mode,
+                                    "n_min": n_min, "n_max": n_max, "batch_min": b_min, "batch_max": b_max,
+                                    "panel": cfg["panel"], "slices": cfg["slices"], "ranges": cfg["ranges"],
+                                    "note": f"n={n} batch={B}: {ms:.3f} ms"})
+                    del ws
+            del Xall
+            torch.cuda.empty_cache()
+    with open(os.path.join(HERE, "tune_table.json")) as f:   # keeps "about" and "defaults"
+        table = json.load(f)
+    table["entries"] = entries
+    table["measured"] = {"device": dev.name, "sms": dev.multi_processor_count,
+                         "torch": torch.__version__, "seconds": round(time.time() - t_start, 1),
+                         "reps": args.reps, "accuracy_margin": args.accuracy_margin}
+    with open(args.out, "w") as f:
+        json.dump(table, f, indent=1)
+        f.write("\n")
+    with open(os.path.splitext(args.out)[0] + "_sweep.json", "w") as f:
+        json.dump(log, f, indent=0)
+    print(json.dumps({"entries": len(entries), "seconds": round(time.time() - t_start, 1)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -123,3 +123,75 @@ def test_graph_capture_replays():
     torch.cuda.synchronize()
     assert torch.equal(plan.log, la0) and torch.equal(plan.sign, sg0)
     check(mats, plan.log, plan.sign)
+
+
+# ------------------------------------------------------------- the large bin
+
+def large_mix(seed):
+    """Orders on both sides of the ragged bin's limit (544), odd ones included,
+    float32 and float64, several matrices of one large order."""
+    rng = np.random.default_rng(seed)
+    orders = [10, 544, 546, 200, 600, 1030, 600, 777, 33, 1200, 600, 2048]
+    mats = []
+    for i, n in enumerate(orders):
+        G = rng.normal(scale=1 / np.sqrt(n), size=(n, n))
+        mats.append(((G - G.T) / 2).astype(np.float32 if i % 3 == 1 else np.float64))
+    return mats
+
+
+def check_any(mats, la, sg):
+    la, sg = la.cpu().numpy(), sg.cpu().numpy()
+    for i, A in enumerate(mats):
+        if A.shape[0] & 1:
+            assert np.isneginf(la[i]) and sg[i] == 0
+            continue
+        wl, ws = O.slog_pf(A)
+        assert abs(la[i] - wl) <= 1e-10 * abs(wl) + 1e-12, (i, A.shape, la[i], wl)
+        assert sg[i] == ws, (i, A.shape)
+
+
+@pytest.mark.parametrize("mode", ["split", "fp64"])
+def test_large_bin_in_the_same_call(mode):
+    """Orders above 544 share the call: each (order, dtype) group runs on the
+    blocked cluster-panel path from the matrices where they lie."""
+    mats = large_mix(21)
+    plan = pf.RaggedPlan([torch.from_numpy(A).cuda() for A in mats], mode=mode)
+    # (546, f64) (600, f32) (600, f64) (1030, f64) (1200, f64) (2048, f64)
+    assert len(plan._groups) == 6
+    la, sg = plan.run()
+    check_any(mats, la, sg)
+
+
+def test_large_bin_graph_capture_replays():
+    mats = large_mix(22)
+    plan = pf.RaggedPlan([torch.from_numpy(A).cuda() for A in mats])
+    la0, sg0 = [x.clone() for x in plan.run()]
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        plan.run()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        plan.run()
+    plan.log.zero_()
+    plan.sign.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    la1, sg1 = plan.log.clone(), plan.sign.clone()
+    # the odd large order keeps the (-inf, 0) written when the plan was built
+    odd = [i for i, A in enumerate(mats) if A.shape[0] & 1 and A.shape[0] > 544]
+    for i in odd:
+        la1[i], sg1[i] = la0[i], sg0[i]
+    assert torch.equal(la1, la0) and torch.equal(sg1, sg0)
+
+
+def test_large_bin_matches_uniform_calls():
+    """Each large group equals a uniform pfb_slog_pfaffian call on the same
+    matrices stacked, bit for bit."""
+    mats = large_mix(23)
+    t = [torch.from_numpy(A).cuda() for A in mats]
+    la, sg = pf.slog_pfaffian_ragged(t)
+    idx = [i for i, A in enumerate(mats) if A.shape[0] == 600 and A.dtype == np.float64]
+    l2, s2 = pf.slog_pfaffian_raw(torch.stack([t[i] for i in idx]), mode="split")
+    assert torch.equal(la[idx], l2) and torch.equal(sg[idx], s2.to(torch.float64))

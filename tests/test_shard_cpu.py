@@ -87,3 +87,63 @@ def test_sharded_gather_world2(cplx):
         assert np.array_equal(la, wl) and np.array_equal(sg, ws)
         lo, hi = shard_range(7, 2, rank)
         assert np.array_equal(own, wl[lo:hi])
+
+
+# ------------------------------------------- ragged, small path, gradients
+
+def _worker_more(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import oracle as O
+        from pfcuda_b200.shard import (slog_pfaffian_ragged_sharded, pfaffian_sharded,
+                                       slog_pfaffian_grad_sharded)
+        rng = np.random.default_rng(9)
+        orders = [8, 40, 100, 34, 200, 12, 66, 150, 90]
+        mats = [torch.from_numpy(O.skew_normal(rng, 1, m, scale=1 / np.sqrt(m))[0]) for m in orders]
+        # other ranks' matrices are placeholders: only their shapes are read
+        plan = shard_ragged(orders, world)
+        given = [M if i in plan[rank] else torch.empty(M.shape, device="meta") for i, M in enumerate(mats)]
+
+        def ragged_compute(lst):
+            la, sg = O.slog_pf_list([M.numpy() for M in lst])
+            return torch.from_numpy(la), torch.from_numpy(sg)
+
+        rl, rs = slog_pfaffian_ragged_sharded(given, compute=ragged_compute)
+        ol, osg, oidx = slog_pfaffian_ragged_sharded(given, compute=ragged_compute, gather=False)
+        S = torch.from_numpy(O.skew_normal(rng, 5, 12))
+        pf_all = pfaffian_sharded(S, compute=lambda X: torch.from_numpy(np.asarray(O.pf_product(X.numpy()))))
+        G = torch.from_numpy(O.skew_normal(rng, 5, 20, scale=0.3))
+        ct = torch.linspace(-1.0, 2.0, 5, dtype=torch.float64)
+        g_all = slog_pfaffian_grad_sharded(
+            G, ct, compute=lambda X, c: torch.from_numpy(O.slog_pf_vjp(X.numpy(), None if c is None else c.numpy())))
+        q.put((rank, rl.numpy(), rs.numpy(), ol.numpy(), oidx.numpy(), pf_all.numpy(), g_all.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_ragged_small_and_grad_world2():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_more, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    from oracle import oracle as O
+    rng = np.random.default_rng(9)
+    orders = [8, 40, 100, 34, 200, 12, 66, 150, 90]
+    mats = [O.skew_normal(rng, 1, m, scale=1 / np.sqrt(m))[0] for m in orders]
+    wl, ws = O.slog_pf_list(mats)
+    S = O.skew_normal(rng, 5, 12)
+    G = O.skew_normal(rng, 5, 20, scale=0.3)
+    plan = shard_ragged(orders, 2)
+    for rank, rl, rs, ol, oidx, pf_all, g_all in got:
+        assert np.array_equal(rl, wl) and np.array_equal(rs, ws)
+        assert list(oidx) == plan[rank] and np.array_equal(ol, wl[plan[rank]])
+        assert np.array_equal(pf_all, O.pf_product(S))
+        assert np.array_equal(g_all, O.slog_pf_vjp(G, np.linspace(-1.0, 2.0, 5)))
