@@ -615,11 +615,15 @@ def main():
 
     # each panel form at the headline batch, split and FP64 (a few calls each)
     forms = {}
+    variants = [("registers", "roundtrip"), ("half_shared", "roundtrip"), ("registers", "reduce"),
+                ("half_shared", "reduce")]
     for m in modes:
-        for form in ("registers", "half_shared"):
+        for form, epi in variants:
             if L.pfb_slog_max_concurrent_form(dtc, n, {"registers": 1, "half_shared": 2}[form]) <= 0:
                 continue
-            cfgx = {"panel": form}
+            if m != "split" and epi != "roundtrip":
+                continue
+            cfgx = {"panel": form, "epilogue": epi}
 
             def stepx(m=m, cfgx=cfgx):
                 pf.slog_pfaffian_raw(A, mode=m, workspace=ws[m], config=cfgx)
@@ -634,7 +638,8 @@ def main():
                 stepx()
             e1.record(stream)
             barrier()
-            forms[f"{m}_{form}_ms"] = max_over_ranks(e0.elapsed_time(e1) / kk)
+            forms[f"{m}_{form}" + (f"_{epi}" if m == "split" else "") + "_ms"] = \
+                max_over_ranks(e0.elapsed_time(e1) / kk)
 
     # accuracy of the headline path against the FP64 oracle (rank 0)
     step(head)

@@ -151,16 +151,28 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
  *           PFB_SPLIT_DIGITS bits, when set, take precedence over the table.
  *   ranges: 1 -- one stream; 2 -- a batch of three or more waves of the widest
  *           panel clusters runs as two ranges (pfb_slog_stream_ranges).
+ *   epilogue (split update, 5 to 7 digits): PFB_EPILOGUE_ROUNDTRIP -- each
+ *           FP64 tile of the working matrix comes into shared memory by TMA,
+ *           is updated there and goes back by TMA; PFB_EPILOGUE_REDUCE -- only
+ *           the tile's increment is formed, and the L2 adds it to the working
+ *           matrix (bulk reduce-add).  Both round identically (one rounding
+ *           of C + increment, the increment exact).
  */
 typedef enum {
     PFB_PANEL_REGISTERS = 1,
     PFB_PANEL_HALF_SHARED = 2
 } pfb_panel_form;
 
+typedef enum {
+    PFB_EPILOGUE_ROUNDTRIP = 1,
+    PFB_EPILOGUE_REDUCE = 2
+} pfb_split_epilogue;
+
 typedef struct {
     int panel;
     int slices;
     int ranges;
+    int epilogue;
 } pfb_slog_config;
 
 /* The configuration a pfb_slog_pfaffian call on these arguments uses (the

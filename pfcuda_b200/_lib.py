@@ -48,14 +48,17 @@ SIGNATURES = {
 
 class SlogConfig(ctypes.Structure):
     """pfb_slog_config of include/pfb200.h (0 fields: the tuned table's choice)."""
-    _fields_ = [("panel", ctypes.c_int), ("slices", ctypes.c_int), ("ranges", ctypes.c_int)]
+    _fields_ = [("panel", ctypes.c_int), ("slices", ctypes.c_int), ("ranges", ctypes.c_int),
+                ("epilogue", ctypes.c_int)]
 
     def as_dict(self):
         return {"panel": {1: "registers", 2: "half_shared"}.get(self.panel, self.panel),
-                "slices": self.slices, "ranges": self.ranges}
+                "slices": self.slices, "ranges": self.ranges,
+                "epilogue": {1: "roundtrip", 2: "reduce"}.get(self.epilogue, self.epilogue)}
 
 
 PANEL_REGISTERS, PANEL_HALF_SHARED = 1, 2
+EPILOGUE_ROUNDTRIP, EPILOGUE_REDUCE = 1, 2
 
 
 class SlogTiming(ctypes.Structure):

@@ -31,6 +31,7 @@ def _nvcc():
 TUNE_JSON = os.path.join(HERE, "tune_table.json")
 TUNE_H = os.path.join(CSRC, "tune_table.h")
 _PANEL = {"registers": 1, "half_shared": 2, 1: 1, 2: 2}
+_EPI = {"roundtrip": 1, "reduce": 2, 1: 1, 2: 2}
 
 
 def write_tune_header() -> str:
@@ -41,11 +42,11 @@ def write_tune_header() -> str:
     d = t["defaults"]
     rows = []
     for e in t["entries"]:
-        rows.append("    {%d, %d, %d, %d, %dLL, %dLL, %d, %d, %d},  // %s" % (
+        rows.append("    {%d, %d, %d, %d, %dLL, %dLL, %d, %d, %d, %d},  // %s" % (
             1 if e["dtype"] == "complex" else 0, 1 if e["mode"] == "split" else 0, e["n_min"], e["n_max"],
             e["batch_min"], e["batch_max"], _PANEL[e["panel"]], e["slices"], e["ranges"],
-            e.get("note", "")))
-    body = "\n".join(rows) if rows else "    {-1, -1, 0, 0, 0LL, 0LL, 0, 0, 0},  // (no measured entries)"
+            _EPI[e.get("epilogue", d["epilogue"])], e.get("note", "")))
+    body = "\n".join(rows) if rows else "    {-1, -1, 0, 0, 0LL, 0LL, 0, 0, 0, 0},  // (no measured entries)"
     text = f"""// tune_table.h -- generated by pfcuda_b200/build.py from pfcuda_b200/tune_table.json
 // (the table pfcuda_b200/tune.py measures); do not edit.
 #pragma once
@@ -58,7 +59,7 @@ namespace pfb {{
 struct TuneEntry {{
     int cplx, split, n_min, n_max;
     long long batch_min, batch_max;
-    int panel, slices, ranges;
+    int panel, slices, ranges, epilogue;
 }};
 
 static const TuneEntry kTuneTable[] = {{
@@ -73,8 +74,8 @@ inline pfb_slog_config tuned_config(int dtype, int n, int64_t batch, bool split)
     for (const TuneEntry &e : kTuneTable)
         if (e.cplx == cplx && e.split == (split ? 1 : 0) && n >= e.n_min && n <= e.n_max &&
             batch >= e.batch_min && batch <= e.batch_max)
-            return pfb_slog_config{{e.panel, e.slices, e.ranges}};
-    return pfb_slog_config{{{_PANEL[d["panel"]]}, {d["slices"]}, {d["ranges"]}}};
+            return pfb_slog_config{{e.panel, e.slices, e.ranges, e.epilogue}};
+    return pfb_slog_config{{{_PANEL[d["panel"]]}, {d["slices"]}, {d["ranges"]}, {_EPI[d["epilogue"]]}}};
 }}
 
 }}  // namespace pfb

@@ -80,7 +80,7 @@ int pfb_slog_max_concurrent(int dtype, int n)
 int pfb_slog_max_concurrent_form(int dtype, int n, int panel)
 {
     if (!valid_dtype(dtype) || n <= 32 || (panel != PFB_PANEL_REGISTERS && panel != PFB_PANEL_HALF_SHARED)) return 0;
-    pfb_slog_config over{panel, 0, 0}, cf;
+    pfb_slog_config over{panel, 0, 0, 0}, cf;
     if (!pfb::large_config(dtype, 1, n, PFB_MODE_FP64, &over, &cf)) return 0;
     return pfb::large_max_concurrent(dtype, n, panel);
 }

@@ -441,6 +441,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
         if (CL > kClusterMax) return PFB_ERR_SIZE;
         const bool use_split = (mode & 0xff) == PFB_MODE_SPLIT && mt > 0;
         sa = split_args(use_split, split_ws, cplx, batch, n, NB, k0, slices);
+        sa.epilogue = cf.epilogue;
         if (mode & PFB_SPLIT_TEST_TIMEOUT) sa.fail_b = 0;
         sa = split_shift(sa, b0);
 
@@ -623,7 +624,7 @@ bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_conf
     if ((mode >> 8) & 0xf) c.slices = (mode >> 8) & 0xf;
     if (over) {
         if (over->panel < 0 || over->panel > 2 || over->slices < 0 || over->slices > kSplitMaxSlices ||
-            over->ranges < 0 || over->ranges > 2)
+            over->ranges < 0 || over->ranges > 2 || over->epilogue < 0 || over->epilogue > 2)
             return false;
         if (over->panel) {
             if (over->panel == PFB_PANEL_HALF_SHARED && !hs_available(dtype, n)) return false;
@@ -631,6 +632,7 @@ bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_conf
         }
         if (over->slices) c.slices = over->slices;
         if (over->ranges) c.ranges = over->ranges;
+        if (over->epilogue) c.epilogue = over->epilogue;
     }
     *out = c;
     return true;

@@ -171,9 +171,13 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
                 const T xh = R[0] * ia;
                 const T yh = rq * ia;
                 // chunks of 4 rows: the compiler barrier keeps it from hoisting
-                // every shared-memory load of the step (register pressure)
+                // every shared-memory load of the step (register pressure);
+                // chunks wholly below row n - 1 are skipped by a branch that is
+                // uniform across the group (k, n are), so the step issues only
+                // the rows it updates -- half of the fixed window on average
 #pragma unroll
                 for (int p0 = 0; p0 < G - 2; p0 += 4) {
+                    if (k + 2 + p0 >= n) break;
 #pragma unroll
                     for (int p = p0; p < p0 + 4 && p < G - 2; p++) {
                         const int r = k + 2 + p;

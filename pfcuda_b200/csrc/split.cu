@@ -32,6 +32,7 @@
 // SplitArgs::err and the kernel frees its TMEM and returns.
 #include <cuda.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <mutex>
 
@@ -83,6 +84,7 @@ SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int 
     int8_t *end = (cplx ? a.ys2 : a.ys) + batch * a.mstride;
     a.ex = reinterpret_cast<int32_t *>(end);
     a.err = a.ex + batch * (int64_t)n;
+    a.epilogue = PFB_EPILOGUE_ROUNDTRIP;
     a.fail_b = -1;
     return a;
 }
@@ -213,6 +215,14 @@ PFB_D void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memor
 PFB_D void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 PFB_D void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 PFB_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// dst[i] += src[i] for `bytes` / 8 doubles, performed by the L2 (an
+// asynchronous bulk reduction from shared memory, tracked by bulk groups)
+PFB_D void bulk_reduce_add_f64(double *dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;"
+                 ::"l"(dst), "r"(src), "r"(bytes) : "memory");
+}
+PFB_D void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 PFB_D void epi_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
 // AND of p over the 512 epilogue threads (a barrier all of them reach), so that
 // a timed-out wait ends the loop of every epilogue thread together
@@ -269,6 +279,13 @@ PFB_D uint32_t cswz(int r, int d)
     return (uint32_t)((d >> 4) * kCBoxBytes + r * 128 + ((((d & 15) >> 1) ^ (r & 7)) << 4));
 }
 
+// The delta tile of the reduce-add epilogue (RED): 128 rows of 64 doubles,
+// row-major with a row stride of 66 doubles (528 bytes: 16-byte aligned rows,
+// and the 16-byte stores of one row per lane fall on all 32 banks per quarter
+// warp).
+constexpr int kDeltaLd = 66;
+constexpr int kDeltaTileBytes = kSplitTileM * kDeltaLd * 8;   // 67,584
+
 // Persistent, warp-specialised update of the upper-triangle (128 x TN) tiles
 // of one matrix's trailing block (blockIdx.y = matrix, blockIdx.x = CTA):
 //   warp 0   bulk copies of the int8 operand chunks,
@@ -292,13 +309,21 @@ PFB_D uint32_t cswz(int r, int d)
 // Epilogue arithmetic: the tile value is 2^(e_a+e_b-56) * sum_l P_l 2^(7(6-l))
 // (fold_levels), added to C with one fused multiply-add.
 //
+// RED (the reduce-add epilogue): C never comes into the SM.  The epilogue
+// writes the tile's increment delta = value * 2^(e_a+e_b-56) (exact: a power
+// of two times a double) into a shared-memory delta tile, and each epilogue
+// warp hands eight of its rows to the L2 as bulk reduce-adds (C += delta, one
+// rounding: the same result as the fused multiply-add).  The C load, the
+// read-modify-write and the store leave the SM's critical path; two delta
+// tiles alternate, one filled while the L2 reads the other.
+//
 // KK (the K of the int8 products) and S (digit slices) are template
 // parameters: with them the MMA issue loop unrolls into constant descriptor
 // offsets.  (A loop with run-time bounds issued one MMA per ~130 cycles on
 // B200, against ~54 unrolled: the issue, not the tensor pipe, was the limit.)
-template <int TN, int NOUT, int KK, int S>
+template <int TN, int NOUT, int KK, int S, bool RED>
 __global__ void __launch_bounds__(kSplitThreads, 1)
-split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int K,
+split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict__ Wd, int n, int k0, int K,
                     MatState *__restrict__ st_all, SplitArgs sa)
 {
     constexpr int TM = kSplitTileM;
@@ -310,8 +335,8 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     constexpr int kk = KK;
     constexpr int a_bytes = TM * kk;            // one slice of the A tile
     constexpr int b_bytes = TN * kk;            // one slice of one B tile
-    unsigned char *sC = smem;                                   // 2 x 64 KB, 1024-aligned
-    unsigned char *sA = sC + 2 * kCTileBytes;
+    unsigned char *sC = smem;                                   // 2 C tiles or 2 delta tiles, 1024-aligned
+    unsigned char *sA = sC + 2 * (RED ? kDeltaTileBytes : kCTileBytes);
     unsigned char *sB = sA + kSplitMaxSlices * a_bytes;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sB + NOUT * kSplitMaxSlices * b_bytes);
     // bars: 0 a_full, 1 a_empty, 2 b_full, 3 b_empty, 4 acc_full, 5 acc_empty, 6-7 c_full
@@ -439,6 +464,90 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
             }
             if (!ok) atomicExch(s_fail, 1);
         }
+    } else if constexpr (RED) {
+        // ---------------- epilogue (warps 2-17), thread = tile row; C += delta in the L2
+        const int quarter = warp & 3;
+        const int h = (warp - 2) >> 2;              // column group: 16 doubles
+        const int r = quarter * 32 + lane;          // row within the tile
+        const int e = warp - 2;                     // this warp hands rows 8e .. 8e+7 to the L2
+        double *Wb = Wd + b * (int64_t)NOUT * n * n;
+        TileWalk tw{ntn, R, 0, 0};
+        tw.start(t1 - 1);
+        for (int it = 0; it < ntiles && ok; it++) {
+            const int buf = it & 1;
+            const int arow = k1 + tw.I * TM + r;
+            const int bc0 = k1 + tw.J * TN + h * CW;
+            const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
+            const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
+            ok = epi_all(mbar_wait_bounded(mb(4), it & 1, lim));
+            if (!ok) break;
+            tc_fence_after();
+            double dv[NOUT][CW];
+#pragma unroll
+            for (int c8 = 0; c8 < CW / 8; c8++) {
+#pragma unroll
+                for (int o = 0; o < NOUT; o++) {
+                    int32_t v[S][8];
+#pragma unroll
+                    for (int l = 0; l < S; l++)
+                        tmem_ld8(tmem + ((uint32_t)(quarter * 32) << 16) +
+                                     (uint32_t)((o * S + l) * TN + h * CW + c8 * 8), v[l]);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        int32_t P[kSplitMaxSlices];
+#pragma unroll
+                        for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l < S ? l : 0][c] : 0;
+                        dv[o][c8 * 8 + c] = fold_levels(P);
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(mb(5));
+            // this delta tile was last read by the reduce-adds of tile it - 2
+            if (lane == 0 && it >= 2) bulk_wait_read1();
+            epi_sync();
+            double *db = reinterpret_cast<double *>(sC + buf * kDeltaTileBytes);
+#pragma unroll
+            for (int c8 = 0; c8 < CW / 8; c8++) {
+                double sc[8];
+#pragma unroll
+                for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
+                const int d0 = h * 16 + c8 * 8 * NOUT;
+#pragma unroll
+                for (int pr = 0; pr < 4 * NOUT; pr++) {
+                    double2 v;
+                    if (NOUT == 1) {
+                        v.x = dv[0][c8 * 8 + 2 * pr] * sc[2 * pr];
+                        v.y = dv[0][c8 * 8 + 2 * pr + 1] * sc[2 * pr + 1];
+                    } else {
+                        v.x = dv[0][c8 * 8 + pr] * sc[pr];
+                        v.y = dv[NOUT - 1][c8 * 8 + pr] * sc[pr];
+                    }
+                    *reinterpret_cast<double2 *>(db + r * kDeltaLd + d0 + 2 * pr) = v;
+                }
+            }
+            fence_proxy_async();
+            epi_sync();
+            if (lane == 0) {
+                const int c0 = k1 + tw.J * TN;
+                const int cols = (n - c0 < TN) ? n - c0 : TN;      // even: n and c0 are
+                const uint32_t bytes = (uint32_t)(cols * NOUT * 8);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int rr = 8 * e + i;
+                    const int a = k1 + tw.I * TM + rr;
+                    if (a < n)
+                        bulk_reduce_add_f64(Wb + (int64_t)a * NOUT * n + (int64_t)NOUT * c0,
+                                            su32(db + rr * kDeltaLd), bytes);
+                }
+                bulk_commit();
+            }
+            tw.step();
+        }
+        // every reduce-add has landed before the CTA exits
+        if (lane == 0) bulk_wait0();
+        if (!ok) atomicExch(s_fail, 1);
     } else {
         // ---------------- epilogue (warps 2-17), thread = tile row
         const bool leader = tid == 64;
@@ -570,10 +679,10 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, int n, int k0, int
     }
 }
 
-template <int TN, int NOUT>
+template <int TN, int NOUT, bool RED>
 static size_t split_smem_bytes(int kk)
 {
-    return (size_t)2 * kCTileBytes + (size_t)kSplitMaxSlices * kSplitTileM * kk +
+    return (size_t)2 * (RED ? kDeltaTileBytes : kCTileBytes) + (size_t)kSplitMaxSlices * kSplitTileM * kk +
            (size_t)NOUT * kSplitMaxSlices * TN * kk + 8 * 8 + 16;
 }
 
@@ -612,7 +721,7 @@ static bool make_c_map(CUtensorMap *map, void *W, int n, int nout, int64_t batch
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int TN, int NOUT, int KK, int S>
+template <int TN, int NOUT, int KK, int S, bool RED>
 static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
                           cudaStream_t stream)
 {
@@ -629,28 +738,39 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     if (per > (tiles + 1) / 2) per = (tiles + 1) / 2;
     if (per < 1) per = 1;
     CUtensorMap map;
-    if (!make_c_map(&map, W, n, NOUT, batch)) return PFB_ERR_UNSUPPORTED;
-    auto k = split_update_kernel<TN, NOUT, KK, S>;
-    const size_t smem = split_smem_bytes<TN, NOUT>(KK);
+    memset(&map, 0, sizeof(map));
+    if (!RED && !make_c_map(&map, W, n, NOUT, batch)) return PFB_ERR_UNSUPPORTED;
+    auto k = split_update_kernel<TN, NOUT, KK, S, RED>;
+    const size_t smem = split_smem_bytes<TN, NOUT, RED>(KK);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PFB_ERR_CUDA;
-    k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(map, n, k0, K, st, sa);
+    k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(map, static_cast<double *>(W), n,
+                                                                            k0, K, st, sa);
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
-// one instantiation per (operand width, slices): the MMA issue unrolls
+// one instantiation per (operand width, slices, epilogue): the MMA issue
+// unrolls; the reduce-add epilogue is built for 5 to 7 digits (the counts the
+// accuracy bar admits), fewer digits use the shared-memory round trip
 template <int TN, int NOUT, int KK>
 static int launch_split_s(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
                           cudaStream_t stream)
 {
+    const bool red = sa.epilogue == PFB_EPILOGUE_REDUCE;
     switch (sa.slices) {
-    case 1: return launch_split_t<TN, NOUT, KK, 1>(W, n, k0, K, batch, st, sa, stream);
-    case 2: return launch_split_t<TN, NOUT, KK, 2>(W, n, k0, K, batch, st, sa, stream);
-    case 3: return launch_split_t<TN, NOUT, KK, 3>(W, n, k0, K, batch, st, sa, stream);
-    case 4: return launch_split_t<TN, NOUT, KK, 4>(W, n, k0, K, batch, st, sa, stream);
-    case 5: return launch_split_t<TN, NOUT, KK, 5>(W, n, k0, K, batch, st, sa, stream);
-    case 6: return launch_split_t<TN, NOUT, KK, 6>(W, n, k0, K, batch, st, sa, stream);
-    case 7: return launch_split_t<TN, NOUT, KK, 7>(W, n, k0, K, batch, st, sa, stream);
+    case 1: return launch_split_t<TN, NOUT, KK, 1, false>(W, n, k0, K, batch, st, sa, stream);
+    case 2: return launch_split_t<TN, NOUT, KK, 2, false>(W, n, k0, K, batch, st, sa, stream);
+    case 3: return launch_split_t<TN, NOUT, KK, 3, false>(W, n, k0, K, batch, st, sa, stream);
+    case 4: return launch_split_t<TN, NOUT, KK, 4, false>(W, n, k0, K, batch, st, sa, stream);
+    case 5:
+        return red ? launch_split_t<TN, NOUT, KK, 5, true>(W, n, k0, K, batch, st, sa, stream)
+                   : launch_split_t<TN, NOUT, KK, 5, false>(W, n, k0, K, batch, st, sa, stream);
+    case 6:
+        return red ? launch_split_t<TN, NOUT, KK, 6, true>(W, n, k0, K, batch, st, sa, stream)
+                   : launch_split_t<TN, NOUT, KK, 6, false>(W, n, k0, K, batch, st, sa, stream);
+    case 7:
+        return red ? launch_split_t<TN, NOUT, KK, 7, true>(W, n, k0, K, batch, st, sa, stream)
+                   : launch_split_t<TN, NOUT, KK, 7, false>(W, n, k0, K, batch, st, sa, stream);
     default: return PFB_ERR_INVALID;
     }
 }

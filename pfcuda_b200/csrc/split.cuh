@@ -34,6 +34,7 @@ struct SplitArgs {
     int8_t *ys2;              // complex only: [Yi | Yr]
     int32_t *ex;              // [B][n] power-of-two exponent per trailing index
     int32_t *err;             // [B] device-side timeout flags of the update kernel
+    int epilogue;             // PFB_EPILOGUE_ROUNDTRIP or PFB_EPILOGUE_REDUCE
     int fail_b;               // matrix (of this range) whose waits give up at once, -1: none
                               // (PFB_SPLIT_TEST_TIMEOUT, which exercises the timeout path)
 };

@@ -10,11 +10,11 @@ namespace pfb {
 struct TuneEntry {
     int cplx, split, n_min, n_max;
     long long batch_min, batch_max;
-    int panel, slices, ranges;
+    int panel, slices, ranges, epilogue;
 };
 
 static const TuneEntry kTuneTable[] = {
-    {-1, -1, 0, 0, 0LL, 0LL, 0, 0, 0},  // (no measured entries)
+    {-1, -1, 0, 0, 0LL, 0LL, 0, 0, 0, 0},  // (no measured entries)
 };
 
 // The first entry for this dtype class and mode whose order and batch bins
@@ -25,8 +25,8 @@ inline pfb_slog_config tuned_config(int dtype, int n, int64_t batch, bool split)
     for (const TuneEntry &e : kTuneTable)
         if (e.cplx == cplx && e.split == (split ? 1 : 0) && n >= e.n_min && n <= e.n_max &&
             batch >= e.batch_min && batch <= e.batch_max)
-            return pfb_slog_config{e.panel, e.slices, e.ranges};
-    return pfb_slog_config{1, 7, 2};
+            return pfb_slog_config{e.panel, e.slices, e.ranges, e.epilogue};
+    return pfb_slog_config{1, 7, 2, 1};
 }
 
 }  // namespace pfb

@@ -15,6 +15,8 @@ Knobs:
           to 4160 real / 2080 complex)
   ranges  1 | 2 (a batch of three or more waves of wide panel clusters split
           over two streams)
+  epilogue  split update: roundtrip (C tile through shared memory) | reduce
+          (the increment added by the L2)
   slices  int8 digits per operand of the split update: 7 always qualifies; 6
           and 5 are kept only where the log error stays within
           --accuracy-margin x 1e-10 relative both on random matrices (against
@@ -141,25 +143,27 @@ def main():
                     ws = torch.empty(pf.slog_workspace_bytes(tdt, B, n, mode), dtype=torch.uint8, device="cuda")
                     panels = ["registers"] + (["half_shared"] if m2 > 0 else [])
                     slices = [7, 6, 5] if mode == "split" else [7]
+                    epis = ["roundtrip", "reduce"] if mode == "split" else ["roundtrip"]
                     best = None
                     for panel in panels:
                         for ranges in (1, 2):
                             for sl in slices:
                                 if sl < 7 and not slices_ok(pf, n, cplx, sl, args.accuracy_margin, acc_cache):
                                     continue
-                                cfg = {"panel": panel, "ranges": ranges, "slices": sl}
-                                ms = time_call(pf, X, mode, cfg, ws, args.reps)
-                                log.append({"dtype": "complex" if cplx else "real", "mode": mode, "n": n,
-                                            "batch": B, **cfg, "ms": ms})
-                                if best is None or ms < best[0]:
-                                    best = (ms, cfg)
+                                for epi in epis:
+                                    cfg = {"panel": panel, "ranges": ranges, "slices": sl, "epilogue": epi}
+                                    ms = time_call(pf, X, mode, cfg, ws, args.reps)
+                                    log.append({"dtype": "complex" if cplx else "real", "mode": mode, "n": n,
+                                                "batch": B, **cfg, "ms": ms})
+                                    if best is None or ms < best[0]:
+                                        best = (ms, cfg)
                     ms, cfg = best
                     print(f"{'c128' if cplx else 'f64'} {mode} n={n} batch={B}: {cfg} {ms:.3f} ms "
                           f"({B / ms * 1e3:.1f} matrices/s)", file=sys.stderr)
                     entries.append({"dtype": "complex" if cplx else "real", "mode": mode,
                                     "n_min": n_min, "n_max": n_max, "batch_min": b_min, "batch_max": b_max,
                                     "panel": cfg["panel"], "slices": cfg["slices"], "ranges": cfg["ranges"],
-                                    "note": f"n={n} batch={B}: {ms:.3f} ms"})
+                                    "epilogue": cfg["epilogue"], "note": f"n={n} batch={B}: {ms:.3f} ms"})
                     del ws
             del Xall
             torch.cuda.empty_cache()

@@ -102,3 +102,36 @@ def test_config_overrides_are_checked():
         pf.slog_pfaffian_raw(X, mode="split", config={"slices": 8})
     cfg = pf.slog_config(torch.float64, 28, 4096, "split")
     assert cfg["panel"] in ("registers", "half_shared") and 1 <= cfg["slices"] <= 7 and cfg["ranges"] in (1, 2)
+
+
+# ------------------------------------------------------ split epilogues
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("n", [34, 66, 130, 256, 514, 1030])
+def test_split_epilogues_equal(cplx, n):
+    """The split update's two epilogues -- the C tile through shared memory
+    (round trip) and the L2 reduce-add of the increment -- round identically:
+    the increment value * 2^e is exact and C + increment is rounded once in
+    both, so results and pivots are equal bit for bit."""
+    rng = np.random.default_rng(700 + n + cplx)
+    A = O.skew_normal(rng, 3, n, scale=1 / np.sqrt(n), complex_=cplx)
+    X = cuda(A)
+    r1 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "roundtrip"})
+    r2 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "reduce"})
+    for a, b in zip(r1, r2):
+        assert torch.equal(a, b)
+    if n <= 256:
+        wl, ws, wp = O.slog_pf(A, with_pivots=True)
+        la, sg, piv = (x.cpu().numpy() for x in r2)
+        assert np.all(np.abs(la - wl) <= 1e-10 * np.abs(wl) + 1e-12)
+        assert np.array_equal(piv, wp)
+
+
+def test_split_epilogues_equal_at_the_headline_order():
+    rng = np.random.default_rng(9)
+    X = cuda(O.skew_normal(rng, 2, 4096, scale=1 / 64))
+    r1 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "roundtrip"})
+    r2 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True,
+                              config={"epilogue": "reduce", "panel": "half_shared"})
+    for a, b in zip(r1, r2):
+        assert torch.equal(a, b)

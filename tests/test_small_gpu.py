@@ -48,8 +48,16 @@ def test_all_orders_and_dtypes(npdt, n):
     A = O.skew_normal(rng, 37, n, complex_=cplx).astype(npdt)   # 37: partial warps
     got = pfaffian_raw_np(A)
     want = O.pf_product(A.astype(np.complex128 if cplx else np.float64))
-    tol = 1e-10 if np.dtype(npdt).itemsize * (1 if not cplx else 0.5) >= 8 else 2e-3
-    assert np.max(rel_err(got, want)) < tol, (n, npdt)
+    if np.dtype(npdt).itemsize * (1 if not cplx else 0.5) >= 8:
+        assert np.max(rel_err(got, want)) < 1e-10, (n, npdt)
+    else:
+        # single precision: a per-matrix bar from the conditioning of each
+        # matrix, 0.5 n eps32 cond_2(A) -- a float32 emulation of the same
+        # elimination on 1600 random matrices per dtype stays below
+        # 0.09 n eps32 cond_2(A); the FP64 oracle runs on the same rounded input
+        eps = np.finfo(np.float32).eps
+        bar = 0.5 * n * eps * np.linalg.cond(A.astype(np.complex128))
+        assert np.all(rel_err(got, want) <= bar), (n, npdt, np.max(rel_err(got, want) / bar))
 
 
 def pfaffian_raw_np(A, layout=_lib.ROW_MAJOR):
