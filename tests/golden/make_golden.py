@@ -1,8 +1,8 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-    python tests/golden/make_golden.py [REFERENCE_TREE]
+    python tests/golden/make_golden.py REFERENCE_TREE
 
-Needs the reference tree (default /root/reference) and the checker libraries
+Needs the reference tree (its path is the one argument) and the checker libraries
 built by oracle/Makefile (oracle/_ref/libref_cpu.so is the reference's own
 src/pfaffian_cpu.cpp).  Outputs, all seeded and reproducible:
 
@@ -104,4 +104,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_TREE")
+    main(sys.argv[1])
