@@ -48,6 +48,10 @@ def parse():
     p.add_argument("--dtype", default="float64", choices=["float64", "complex128"])
     p.add_argument("--mode", default="auto", choices=["auto", "split", "fp64"])
     p.add_argument("--batch", type=int, default=0, help="matrices per call (0: four waves of concurrently resident panel clusters)")
+    p.add_argument("--panel", default="table", choices=["table", "registers", "half_shared"],
+                   help="panel form of the headline calls (table: the tuned table's choice)")
+    p.add_argument("--epilogue", default="table", choices=["table", "roundtrip", "reduce"],
+                   help="split-update epilogue of the headline calls (table: the tuned table's choice)")
     p.add_argument("--workloads", default="all",
                    choices=["all", "headline", "small", "ragged", "grad", "illcond"],
                    help="'all': the headline line plus the other workloads under 'workloads'; "
@@ -568,10 +572,16 @@ def main():
     la = torch.empty(B, dtype=torch.float64, device=dev)
     sg = torch.empty(B, dtype=tdt, device=dev)
 
+    # the configuration overrides given on the command line (0: the tuned table's choice)
+    over = _lib.SlogConfig({"table": 0, "registers": 1, "half_shared": 2}[args.panel], 0, 0,
+                           {"table": 0, "roundtrip": 1, "reduce": 2}[args.epilogue])
+    over_p = ctypes.byref(over) if (over.panel or over.epilogue) else None
+
     def step(mode, src=None, nb=B):
         X = src if src is not None else A
-        st = L.pfb_slog_pfaffian(dtc, X.data_ptr(), nb, n, _lib.ROW_MAJOR, mc[mode], la.data_ptr(),
-                                 sg.data_ptr(), ws[mode].data_ptr(), ws[mode].numel(), stream.cuda_stream)
+        st = L.pfb_slog_pfaffian_ex(dtc, X.data_ptr(), nb, n, _lib.ROW_MAJOR, mc[mode], la.data_ptr(),
+                                    sg.data_ptr(), ws[mode].data_ptr(), ws[mode].numel(), stream.cuda_stream,
+                                    None, over_p)
         _lib.check(st, "pfb_slog_pfaffian")
 
     def barrier():
@@ -666,10 +676,10 @@ def main():
     arr = [(ctypes.c_void_p * (2 * npan))(*[e.cuda_event for e in es]) for es in evs]
     tm = _lib.SlogTiming(ctypes.cast(arr[0], ctypes.POINTER(ctypes.c_void_p)),
                          ctypes.cast(arr[1], ctypes.POINTER(ctypes.c_void_p)), npan)
-    st = L.pfb_slog_pfaffian_timed(dtc, A.data_ptr(), B, n, _lib.ROW_MAJOR, mc[head], la.data_ptr(),
-                                   sg.data_ptr(), ws[head].data_ptr(), ws[head].numel(),
-                                   stream.cuda_stream, ctypes.byref(tm))
-    _lib.check(st, "pfb_slog_pfaffian_timed")
+    st = L.pfb_slog_pfaffian_ex(dtc, A.data_ptr(), B, n, _lib.ROW_MAJOR, mc[head], la.data_ptr(),
+                                sg.data_ptr(), ws[head].data_ptr(), ws[head].numel(),
+                                stream.cuda_stream, ctypes.byref(tm), over_p)
+    _lib.check(st, "pfb_slog_pfaffian_ex (timed)")
     torch.cuda.synchronize()
     panel_ms = sum(evs[0][2 * i].elapsed_time(evs[0][2 * i + 1]) for i in range(npan))
     upd_ms = sum(evs[1][2 * i].elapsed_time(evs[1][2 * i + 1]) for i in range(npan - 1))
@@ -771,6 +781,7 @@ def main():
                    "l2": f"inputs {B * n * n * esz / 1e6:.0f} MB > 126 MB L2, re-read every step",
                    "parallelism": f"replicas x{world}"},
         "tuned_config": tuned,
+        "config_override": {"panel": args.panel, "epilogue": args.epilogue},
         "tuned_config_batch1": tuned1,
         "panel_forms_ms_per_step": forms,
         "modes_ms_per_step": results,
