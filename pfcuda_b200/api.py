@@ -84,14 +84,40 @@ def pfaffian(A):
     return _out(_PfaffianFn.apply(A.contiguous()), as_np)
 
 
-def resolve_mode(mode: str, dtype: torch.dtype) -> str:
-    """"auto" -> the faster trailing update on B200 for this dtype: "split"
-    for real inputs, "fp64" for complex ones (the FP64 tensor-core update beats
-    the complex split update, whose int8 products are twice as deep: at 2n =
-    2048 complex128, 42.3 against 48.3 ms per 59 matrices; at 2n = 4096 the two
-    are within 2%, and FP64 is exact in the update)."""
+_TUNED = None
+
+
+def _tuned_entries():
+    """The measured entries of pfcuda_b200/tune_table.json (loaded once)."""
+    global _TUNED
+    if _TUNED is None:
+        import json
+        import os
+        try:
+            with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tune_table.json")) as f:
+                _TUNED = json.load(f).get("entries", [])
+        except (OSError, ValueError):
+            _TUNED = []
+    return _TUNED
+
+
+def resolve_mode(mode: str, dtype: torch.dtype, n: int | None = None, batch: int | None = None) -> str:
+    """"auto" -> the faster trailing update for this dtype class, order and
+    batch by the tuned table's measurements (both modes meet the 1e-10 bar on
+    log|Pf|), else the defaults: "split" for real inputs, "fp64" for complex
+    ones (the complex split update's int8 products are twice as deep)."""
     if mode == "auto":
-        return "fp64" if dtype in (torch.complex64, torch.complex128) else "split"
+        cplx = dtype in (torch.complex64, torch.complex128)
+        if n is not None and batch is not None:
+            cls = "complex" if cplx else "real"
+            ms = {}
+            for e in _tuned_entries():
+                if (e.get("dtype") == cls and e["n_min"] <= n <= e["n_max"]
+                        and e["batch_min"] <= batch <= e["batch_max"] and "ms" in e):
+                    ms.setdefault(e["mode"], e["ms"])
+            if "split" in ms and "fp64" in ms:
+                return "split" if ms["split"] <= ms["fp64"] else "fp64"
+        return "fp64" if cplx else "split"
     if mode not in _MODES:
         raise ValueError(f"mode must be 'auto' or one of {sorted(_MODES)}")
     return mode
@@ -105,7 +131,8 @@ def slog_pfaffian(A, mode: str = "auto"):
     has A's dtype (a unit-modulus phase for complex A, 0 when Pf = 0).
     ``mode`` picks the arithmetic of the trailing update: "split" (int8 slices on
     the tensor cores, recombined in FP64), "fp64" (the FP64 tensor cores), or
-    "auto" (resolve_mode: split for real inputs, fp64 for complex ones).
+    "auto" (resolve_mode: the faster of the two by the tuned table's
+    measurements for this dtype, order and batch).
     """
     A, as_np = _prep(A)
     n = A.shape[-1]
@@ -117,7 +144,7 @@ def slog_pfaffian(A, mode: str = "auto"):
         la = torch.full(lead, -float("inf"), dtype=torch.float64, device=A.device)
         sg = torch.zeros(lead, dtype=A.dtype, device=A.device)
         return _out(la, as_np), _out(sg, as_np)
-    mode = resolve_mode(mode, A.dtype)
+    mode = resolve_mode(mode, A.dtype, n, int(np.prod(A.shape[:-2])) if A.ndim > 2 else 1)
     A = _to_device(A, as_np)
     la, sg = _SlogFn.apply(A.contiguous(), mode)
     return _out(la, as_np), _out(sg, as_np)
@@ -234,7 +261,8 @@ class RaggedPlan:
     a device-side sort, largest first, and an atomic work queue, every matrix
     factored in FP64); larger orders -- the large bin -- go to the blocked
     cluster-panel path, one pfb_slog_pfaffian_ptrs call per (order, dtype) on
-    the matrices where they lie, in ``mode`` ("auto": split-precision update).
+    the matrices where they lie, in ``mode`` ("auto": per group, the faster
+    update by the tuned table).
     The device arrays of pointers, orders and dtypes, the workspaces and the
     index maps are built here; ``run()`` enqueues everything on the current
     stream and returns (log|Pf|, sign) as float64 tensors in the input order.
@@ -257,7 +285,7 @@ class RaggedPlan:
         self.mats = [M.contiguous() for M in mats]
         self.count = len(self.mats)
         self.layout = layout
-        self.mode = resolve_mode(mode, torch.float64)
+        self.mode = mode
         orders = [M.shape[0] for M in self.mats]
         self.max_n = max(orders)
         small = [i for i, m in enumerate(orders) if m <= self.RAGGED_MAX_N]
@@ -303,11 +331,12 @@ class RaggedPlan:
             # float32 signs are widened through a preallocated buffer
             sgd = sg if dt == torch.float64 else torch.empty(len(idx), dtype=torch.float64, device=dev)
             it = torch.tensor(idx, dtype=torch.int64, device=dev)
-            wsb = int(L.pfb_slog_workspace_bytes(_DT[dt], len(idx), m, _MODES[self.mode]))
+            gm = resolve_mode(mode, dt, m, len(idx))
+            wsb = int(L.pfb_slog_workspace_bytes(_DT[dt], len(idx), m, _MODES[gm]))
             if wsb == 0:
                 raise ValueError(f"order {m} is beyond the large path")
             wmax = max(wmax, wsb)
-            self._groups.append((m, dt, ptrs, lg, sg, sgd, it, wsb))
+            self._groups.append((m, dt, gm, ptrs, lg, sg, sgd, it, wsb))
         self._ws_large = torch.empty(max(wmax, 1), dtype=torch.uint8, device=dev) if self._groups else None
 
     @property
@@ -318,11 +347,11 @@ class RaggedPlan:
         k = 2 if self._small else 0
         if self._small and not self._direct:
             k += 2
-        for (m, dt, ptrs, lg, sg, sgd, it, wsb) in self._groups:
+        for (m, dt, gm, ptrs, lg, sg, sgd, it, wsb) in self._groups:
             nb = int(L.pfb_slog_panel_width(_DT[dt], m))
             npan = (m - 1 + nb - 1) // nb
-            per = 2 + npan + (npan - 1) * (2 if self.mode == "split" else 1)
-            k += per * int(L.pfb_slog_stream_ranges(_DT[dt], ptrs.numel(), m, _MODES[self.mode]))
+            per = 2 + npan + (npan - 1) * (2 if gm == "split" else 1)
+            k += per * int(L.pfb_slog_stream_ranges(_DT[dt], ptrs.numel(), m, _MODES[gm]))
             k += 2 + (0 if sgd is sg else 1)
         return k
 
@@ -338,9 +367,9 @@ class RaggedPlan:
             if not self._direct:
                 self.log.index_copy_(0, self._idx_s, self._log_s)
                 self.sign.index_copy_(0, self._idx_s, self._sign_s)
-        for (m, dt, ptrs, lg, sg, sgd, it, wsb) in self._groups:
+        for (m, dt, gm, ptrs, lg, sg, sgd, it, wsb) in self._groups:
             st = L.pfb_slog_pfaffian_ptrs(_DT[dt], ptrs.data_ptr(), ptrs.numel(), m, self.layout,
-                                          _MODES[self.mode], lg.data_ptr(), sg.data_ptr(),
+                                          _MODES[gm], lg.data_ptr(), sg.data_ptr(),
                                           self._ws_large.data_ptr(), wsb, stream)
             _lib.check(st, "pfb_slog_pfaffian_ptrs")
             if sgd is not sg:

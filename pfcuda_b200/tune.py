@@ -163,7 +163,8 @@ def main():
                     entries.append({"dtype": "complex" if cplx else "real", "mode": mode,
                                     "n_min": n_min, "n_max": n_max, "batch_min": b_min, "batch_max": b_max,
                                     "panel": cfg["panel"], "slices": cfg["slices"], "ranges": cfg["ranges"],
-                                    "epilogue": cfg["epilogue"], "note": f"n={n} batch={B}: {ms:.3f} ms"})
+                                    "epilogue": cfg["epilogue"], "ms": round(ms, 4),
+                                    "note": f"n={n} batch={B}: {ms:.3f} ms"})
                     del ws
             del Xall
             torch.cuda.empty_cache()

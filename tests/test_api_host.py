@@ -66,3 +66,21 @@ def test_mode_resolution():
         pf.resolve_mode("tf32", torch.float64)
     with pytest.raises(ValueError, match="mode"):
         pf.slog_pfaffian(torch.zeros(40, 40, dtype=torch.float64), mode="tf32")
+
+
+def test_auto_mode_follows_the_tuned_table(monkeypatch):
+    """With measured entries for both modes, "auto" takes the faster one for
+    the dtype class, order bin and batch bin; without, the defaults."""
+    import pfcuda_b200.api as api
+    entries = [
+        {"dtype": "complex", "mode": "split", "n_min": 1058, "n_max": 2080, "batch_min": 2, "batch_max": 50, "ms": 30.0},
+        {"dtype": "complex", "mode": "fp64", "n_min": 1058, "n_max": 2080, "batch_min": 2, "batch_max": 50, "ms": 40.0},
+        {"dtype": "real", "mode": "split", "n_min": 34, "n_max": 544, "batch_min": 1, "batch_max": 1, "ms": 2.0},
+        {"dtype": "real", "mode": "fp64", "n_min": 34, "n_max": 544, "batch_min": 1, "batch_max": 1, "ms": 1.5},
+    ]
+    monkeypatch.setattr(api, "_TUNED", entries)
+    assert api.resolve_mode("auto", torch.complex128, 2048, 10) == "split"
+    assert api.resolve_mode("auto", torch.complex128, 4096, 10) == "fp64"      # no entry: default
+    assert api.resolve_mode("auto", torch.float64, 512, 1) == "fp64"
+    assert api.resolve_mode("auto", torch.float64, 512, 7) == "split"          # no entry: default
+    assert api.resolve_mode("fp64", torch.float64, 512, 7) == "fp64"

@@ -193,10 +193,12 @@ def test_max_concurrent_query():
 
 
 def test_auto_mode_picks_per_dtype():
-    """slog_pfaffian's default mode: split for real inputs, fp64 for complex."""
+    """slog_pfaffian's default mode is the one resolve_mode picks from the
+    tuned table for the dtype, order and batch."""
     rng = np.random.default_rng(31)
-    for cplx, want in ((False, "split"), (True, "fp64")):
+    for cplx in (False, True):
         A = cuda(O.skew_normal(rng, 2, 130, scale=1 / np.sqrt(130), complex_=cplx))
+        want = pf.resolve_mode("auto", A.dtype, 130, 2)
         la, sg = pf.slog_pfaffian(A)
         lw, sw = pf.slog_pfaffian(A, mode=want)
         assert torch.equal(la, lw) and torch.equal(sg, sw)

@@ -193,5 +193,6 @@ def test_large_bin_matches_uniform_calls():
     t = [torch.from_numpy(A).cuda() for A in mats]
     la, sg = pf.slog_pfaffian_ragged(t)
     idx = [i for i, A in enumerate(mats) if A.shape[0] == 600 and A.dtype == np.float64]
-    l2, s2 = pf.slog_pfaffian_raw(torch.stack([t[i] for i in idx]), mode="split")
+    gm = pf.resolve_mode("auto", torch.float64, 600, len(idx))
+    l2, s2 = pf.slog_pfaffian_raw(torch.stack([t[i] for i in idx]), mode=gm)
     assert torch.equal(la[idx], l2) and torch.equal(sg[idx], s2.to(torch.float64))
