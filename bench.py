@@ -491,6 +491,20 @@ def _hbm_peak():
         return 6650.0
 
 
+def _hbm_peak_source():
+    try:
+        json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        return "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, ValueError, KeyError):
+        return "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
+
+
+# DRAM read+write bytes over algorithmic bytes per launch for kernels captured
+# with ncu after the first captures quoted at the roofline block below
+# (filled from the profiles of this engine's later kernels; None: not captured)
+TRAFFIC_RATIO_MEASURED = {}
+
+
 def auto_batch(n, dtype="float64"):
     """The saturating batch: four waves of the widest panel clusters (one
     cluster per matrix; pfb_slog_max_concurrent of them resident at once), at
@@ -753,24 +767,35 @@ def main():
     # gemm_dmma_kernel at k0 = 320 (177 / 175 MB against 228 MB: part of the
     # written tiles is still in L2 when the launch ends)
     traffic_ratio = {"panel_kernel": 2.39, "split_update_kernel": 0.78, "gemm_dmma_kernel": 0.77}
+    traffic_ratio.update(TRAFFIC_RATIO_MEASURED)
+    # the configuration the headline call ran: the command line's override, else the table's
+    eff = dict(tuned[head])
+    if args.panel != "table":
+        eff["panel"] = args.panel
+    if args.epilogue != "table":
+        eff["epilogue"] = args.epilogue
+    pk_name = "panel_hs_kernel" if eff["panel"] == "half_shared" else "panel_kernel"
     if dominant == "panel":
         achieved = panel_bytes / (panel_ms * 1e-3) / 1e9
-        roof = {"kernel": "panel_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+        tr = traffic_ratio.get(pk_name)
+        roof = {"kernel": pk_name, "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": traffic_ratio["panel_kernel"] * panel_bytes / npan,
+                "traffic": tr * panel_bytes / npan if tr else None,
                 "note": "latency-bound: 32 dependent pivot steps per launch, each a cluster barrier and a "
                         "global load of the interchanged row (~7k cycles per step); algorithmic bytes = "
                         "panel rows read and written once; traffic per launch scaled from ncu"}
     else:
         kname = "split_update_kernel" if head == "split" else "gemm_dmma_kernel"
+        tkey = kname + ("_reduce" if head == "split" and eff.get("epilogue") == "reduce" else "")
         achieved = upd_bytes / (upd_ms * 1e-3) / 1e9
-        roof = {"kernel": kname, "bound": "hbm",
+        tr = traffic_ratio.get(tkey)
+        roof = {"kernel": kname, "variant": tkey, "bound": "hbm",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": traffic_ratio[kname] * upd_bytes / max(npan - 1, 1),
+                "traffic": tr * upd_bytes / max(npan - 1, 1) if tr else None,
                 "note": "algorithmic bytes = FP64 read+write of the upper trailing block per launch; the "
                         "timed region includes the operand-slicing launch before each update; traffic per "
                         "launch scaled from ncu"}
-    roof["peak_source"] = "MEASURED_PEAKS.json hbm_gbs (measured)"
+    roof["peak_source"] = _hbm_peak_source()
     line = {
         "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
