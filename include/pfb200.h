@@ -149,7 +149,7 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
  *           Both forms choose the same pivots and round identically.
  *   slices: int8 digits per operand of the split update (1..7); the mode's
  *           PFB_SPLIT_DIGITS bits, when set, take precedence over the table.
- *   ranges: 1 -- one stream; 2 -- a batch of three or more waves of the widest
+ *   ranges: 1 -- one stream; 2 -- a batch of two or more waves of the widest
  *           panel clusters runs as two ranges (pfb_slog_stream_ranges).
  *   epilogue (split update, 5 to 7 digits): PFB_EPILOGUE_ROUNDTRIP -- each
  *           FP64 tile of the working matrix comes into shared memory by TMA,
@@ -211,11 +211,11 @@ int pfb_slog_max_concurrent_form(int dtype, int n, int panel);
 /*
  * How many ranges a pfb_slog_pfaffian call on `batch` matrices of order n runs
  * as (1 or 2), for the tuned table's configuration in `mode` (PFB_MODE_*).  When
- * the configuration asks for two ranges, a batch of three or more waves of the
- * widest panel clusters (clusters of 9 or more CTAs) is split in two: the last wave's worth of
- * matrices runs on a second stream that forks from and joins `stream` through
- * events, so its trailing updates fill the SMs the first range's panel waves
- * leave idle.  The second stream belongs to the calling host thread (one per
+ * the configuration asks for two ranges and the widest panel clusters have 9 or
+ * more CTAs, a batch of three or more waves of them is split in two -- the last
+ * wave's worth of matrices on a second stream -- and a batch of two waves into
+ * halves; the second stream forks from and joins `stream` through events, so
+ * one range's trailing updates fill the SMs the other's panel waves leave idle.  The second stream belongs to the calling host thread (one per
  * thread and device, created on its first use and destroyed when the thread
  * exits), so calls from different threads never share it; a call whose
  * thread's second stream is part of another graph capture runs as one range.

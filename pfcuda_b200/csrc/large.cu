@@ -638,18 +638,21 @@ bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_conf
     return true;
 }
 
-// The size of the second range (0: one range) for a call on `batch` matrices:
-// the last wave's worth of the widest panel clusters, when the configuration
-// asks for two ranges and the batch holds three waves or more of clusters of
-// 9 or more CTAs.
+// The size of the second range (0: one range) for a call on `batch` matrices,
+// when the configuration asks for two ranges and the widest panel clusters
+// have 9 or more CTAs: the last wave's worth of them for a batch of three waves
+// or more, half the batch for a batch of two waves or more.
 int64_t large_second_range(int dtype, int64_t batch, int n, const pfb_slog_config &cf)
 {
     int nb = 0, cpt = 0;
     if (cf.ranges != 2 || !large_cfg(dtype, n, &nb, &cpt)) return 0;
     const int widest = (n - nb + kTT * cpt - 1) / (kTT * cpt);
     if (widest < 9) return 0;
-    const int mc = large_max_concurrent(dtype, n, cf.panel);
-    return (mc > 0 && batch >= 3 * (int64_t)mc) ? mc : 0;
+    const int64_t mc = large_max_concurrent(dtype, n, cf.panel);
+    if (mc <= 0) return 0;
+    if (batch >= 3 * mc) return mc;
+    if (batch >= 2 * mc) return batch / 2;
+    return 0;
 }
 
 int launch_large(int dtype, const void *A, int64_t batch, int n, int layout, int mode,
