@@ -235,12 +235,14 @@ def test_two_stream_batches_match_single_ranges(mode):
     assert np.all(np.abs(got - wl) <= 1e-10 * np.abs(wl)) and np.array_equal(sg[-2:].cpu().numpy(), ws)
 
 
+# the register panel form with two ranges: a three-wave batch runs on two streams
+TWO = {"panel": "registers", "ranges": 2}
+
+
 def _two_range_batch(seed):
     n = 2176
     mc = _lib.lib().pfb_slog_max_concurrent(_lib.F64, n)
-    B = 3 * mc
-    if _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n, _lib.MODE_SPLIT) != 2:
-        pytest.skip("the tuned table runs this batch on one stream")
+    B = 3 * mc                                 # three waves of the register form's clusters
     rng = np.random.default_rng(seed)
     return cuda(O.skew_normal(rng, B, n, scale=1 / np.sqrt(n)))
 
@@ -251,7 +253,7 @@ def test_two_threads_call_at_once():
     one of the same call made alone, bit for bit."""
     import threading
     ins = [_two_range_batch(90 + i) for i in range(2)]
-    alone = [pf.slog_pfaffian_raw(X, mode="split") for X in ins]
+    alone = [pf.slog_pfaffian_raw(X, mode="split", config=TWO) for X in ins]
     torch.cuda.synchronize()
     out = [None, None]
     errs = []
@@ -260,7 +262,7 @@ def test_two_threads_call_at_once():
         try:
             s = torch.cuda.Stream()
             with torch.cuda.stream(s):
-                res = [pf.slog_pfaffian_raw(ins[i], mode="split") for _ in range(3)]
+                res = [pf.slog_pfaffian_raw(ins[i], mode="split", config=TWO) for _ in range(3)]
             s.synchronize()
             out[i] = res
         except Exception as e:          # surfaced on the main thread below
@@ -284,11 +286,11 @@ def test_graph_capture_of_two_ranges():
     n, B = X.shape[-1], X.shape[0]
     wsb = pf.slog_workspace_bytes(X.dtype, B, n, "split")
     ws = torch.empty(wsb, dtype=torch.uint8, device=X.device)
-    want = pf.slog_pfaffian_raw(X, mode="split", workspace=ws)
+    want = pf.slog_pfaffian_raw(X, mode="split", workspace=ws, config=TWO)
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.graph(g):
-        la, sg = pf.slog_pfaffian_raw(X, mode="split", workspace=ws)
+        la, sg = pf.slog_pfaffian_raw(X, mode="split", workspace=ws, config=TWO)
     for _ in range(2):
         la.zero_()
         g.replay()
