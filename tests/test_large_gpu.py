@@ -16,6 +16,8 @@ from golden_io import load, split
 pytestmark = pytest.mark.gpu
 
 MODES = ["fp64", "split"]
+# the register panel form with two ranges: a three-wave batch runs on two streams
+TWO = {"panel": "registers", "ranges": 2}
 
 
 def cuda(a):
@@ -217,26 +219,21 @@ def test_two_stream_batches_match_single_ranges(mode):
     # the call under test does run as two ranges, and a one-wave call as one
     m = _lib.MODE_SPLIT if mode == "split" else _lib.MODE_FP64
     cfg = pf.slog_config(torch.float64, B, n, mode)
-    if cfg["ranges"] != 2:
-        pytest.skip(f"the tuned table runs this batch on one stream ({cfg})")
-    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n, m) == 2
-    assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, 2 * mc, n, m) == 2     # halves
+    if cfg["ranges"] == 2 and cfg["panel"] == "registers":
+        assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, B, n, m) == 2
+        assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, 2 * mc, n, m) == 2     # halves
     assert _lib.lib().pfb_slog_stream_ranges(_lib.F64, mc, n, m) == 1
     rng = np.random.default_rng(77)
     A = O.skew_normal(rng, B, n, scale=1 / np.sqrt(n))
     At = cuda(A)
-    la, sg = pf.slog_pfaffian_raw(At, mode=mode)
-    parts = [pf.slog_pfaffian_raw(At[i:i + mc].contiguous(), mode=mode) for i in range(0, B, mc)]
+    la, sg = pf.slog_pfaffian_raw(At, mode=mode, config=TWO)
+    parts = [pf.slog_pfaffian_raw(At[i:i + mc].contiguous(), mode=mode, config=TWO) for i in range(0, B, mc)]
     la1 = torch.cat([p[0] for p in parts])
     sg1 = torch.cat([p[1] for p in parts])
     assert torch.equal(la, la1) and torch.equal(sg, sg1)
     wl, ws = O.slog_pf(A[-2:])
     got = la[-2:].cpu().numpy()
     assert np.all(np.abs(got - wl) <= 1e-10 * np.abs(wl)) and np.array_equal(sg[-2:].cpu().numpy(), ws)
-
-
-# the register panel form with two ranges: a three-wave batch runs on two streams
-TWO = {"panel": "registers", "ranges": 2}
 
 
 def _two_range_batch(seed):
