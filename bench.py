@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--batch", type=int, default=0, help="matrices per call (0: four waves of concurrently resident panel clusters)")
     p.add_argument("--panel", default="table", choices=["table", "registers", "half_shared"],
                    help="panel form of the headline calls (table: the tuned table's choice)")
-    p.add_argument("--epilogue", default="table", choices=["table", "roundtrip", "reduce"],
+    p.add_argument("--epilogue", default="table", choices=["table", "roundtrip", "reduce", "direct"],
                    help="split-update epilogue of the headline calls (table: the tuned table's choice)")
     p.add_argument("--workloads", default="all",
                    choices=["all", "headline", "small", "ragged", "grad", "illcond"],
@@ -588,7 +588,7 @@ def main():
 
     # the configuration overrides given on the command line (0: the tuned table's choice)
     over = _lib.SlogConfig({"table": 0, "registers": 1, "half_shared": 2}[args.panel], 0, 0,
-                           {"table": 0, "roundtrip": 1, "reduce": 2}[args.epilogue])
+                           {"table": 0, "roundtrip": 1, "reduce": 2, "direct": 3}[args.epilogue])
     over_p = ctypes.byref(over) if (over.panel or over.epilogue) else None
 
     def step(mode, src=None, nb=B):
@@ -640,12 +640,14 @@ def main():
     # each panel form at the headline batch, split and FP64 (a few calls each)
     forms = {}
     variants = [("registers", "roundtrip"), ("half_shared", "roundtrip"), ("registers", "reduce"),
-                ("half_shared", "reduce")]
+                ("half_shared", "reduce"), ("registers", "direct"), ("half_shared", "direct")]
     for m in modes:
         for form, epi in variants:
             if L.pfb_slog_max_concurrent_form(dtc, n, {"registers": 1, "half_shared": 2}[form]) <= 0:
                 continue
             if m != "split" and epi != "roundtrip":
+                continue
+            if epi == "direct" and tdt != torch.float64:
                 continue
             cfgx = {"panel": form, "epilogue": epi}
 
@@ -786,7 +788,8 @@ def main():
                         "panel rows read and written once; traffic per launch scaled from ncu"}
     else:
         kname = "split_update_kernel" if head == "split" else "gemm_dmma_kernel"
-        tkey = kname + ("_reduce" if head == "split" and eff.get("epilogue") == "reduce" else "")
+        tkey = kname + (f"_{eff.get('epilogue')}" if head == "split" and eff.get("epilogue") != "roundtrip"
+                        else "")
         achieved = upd_bytes / (upd_ms * 1e-3) / 1e9
         tr = traffic_ratio.get(tkey)
         roof = {"kernel": kname, "variant": tkey, "bound": "hbm",

@@ -155,8 +155,13 @@ int pfb_slog_pfaffian_timed(int dtype, const void *A, int64_t batch, int n, int 
  *           FP64 tile of the working matrix comes into shared memory by TMA,
  *           is updated there and goes back by TMA; PFB_EPILOGUE_REDUCE -- only
  *           the tile's increment is formed, and the L2 adds it to the working
- *           matrix (bulk reduce-add).  Both round identically (one rounding
- *           of C + increment, the increment exact).
+ *           matrix (bulk reduce-add); PFB_EPILOGUE_DIRECT (real
+ *           input; complex input takes the round trip) -- each tile is formed
+ *           transposed, so that the lanes of a warp hold adjacent columns of
+ *           C, which is then read and written straight from global memory in
+ *           coalesced row segments (only the strictly upper part is
+ *           written).  All three round identically: one rounding of
+ *           C + increment, the increment exact.
  */
 typedef enum {
     PFB_PANEL_REGISTERS = 1,
@@ -165,7 +170,8 @@ typedef enum {
 
 typedef enum {
     PFB_EPILOGUE_ROUNDTRIP = 1,
-    PFB_EPILOGUE_REDUCE = 2
+    PFB_EPILOGUE_REDUCE = 2,
+    PFB_EPILOGUE_DIRECT = 3
 } pfb_split_epilogue;
 
 typedef struct {

@@ -54,11 +54,11 @@ class SlogConfig(ctypes.Structure):
     def as_dict(self):
         return {"panel": {1: "registers", 2: "half_shared"}.get(self.panel, self.panel),
                 "slices": self.slices, "ranges": self.ranges,
-                "epilogue": {1: "roundtrip", 2: "reduce"}.get(self.epilogue, self.epilogue)}
+                "epilogue": {1: "roundtrip", 2: "reduce", 3: "direct"}.get(self.epilogue, self.epilogue)}
 
 
 PANEL_REGISTERS, PANEL_HALF_SHARED = 1, 2
-EPILOGUE_ROUNDTRIP, EPILOGUE_REDUCE = 1, 2
+EPILOGUE_ROUNDTRIP, EPILOGUE_REDUCE, EPILOGUE_DIRECT = 1, 2, 3
 
 
 class SlogTiming(ctypes.Structure):

@@ -168,14 +168,15 @@ def slog_workspace_bytes(dtype: torch.dtype, batch: int, n: int, mode: str = "sp
 
 def _config(config):
     """A pfb_slog_config from a dict (panel: "registers" | "half_shared" | 1 | 2,
-    slices: 1..7, ranges: 1 | 2, epilogue: "roundtrip" | "reduce" | 1 | 2;
+    slices: 1..7, ranges: 1 | 2, epilogue: "roundtrip" | "reduce" | "direct" | 1..3;
     missing keys take the tuned table's choice)."""
     if config is None:
         return None
     panel = config.get("panel", 0)
     panel = {"registers": _lib.PANEL_REGISTERS, "half_shared": _lib.PANEL_HALF_SHARED}.get(panel, panel)
     epi = config.get("epilogue", 0)
-    epi = {"roundtrip": _lib.EPILOGUE_ROUNDTRIP, "reduce": _lib.EPILOGUE_REDUCE}.get(epi, epi)
+    epi = {"roundtrip": _lib.EPILOGUE_ROUNDTRIP, "reduce": _lib.EPILOGUE_REDUCE,
+           "direct": _lib.EPILOGUE_DIRECT}.get(epi, epi)
     return _lib.SlogConfig(int(panel), int(config.get("slices", 0)), int(config.get("ranges", 0)), int(epi))
 
 

@@ -31,7 +31,7 @@ def _nvcc():
 TUNE_JSON = os.path.join(HERE, "tune_table.json")
 TUNE_H = os.path.join(CSRC, "tune_table.h")
 _PANEL = {"registers": 1, "half_shared": 2, 1: 1, 2: 2}
-_EPI = {"roundtrip": 1, "reduce": 2, 1: 1, 2: 2}
+_EPI = {"roundtrip": 1, "reduce": 2, "direct": 3, 1: 1, 2: 2, 3: 3}
 
 
 def write_tune_header() -> str:

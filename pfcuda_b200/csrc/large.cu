@@ -624,7 +624,7 @@ bool large_config(int dtype, int64_t batch, int n, int mode, const pfb_slog_conf
     if ((mode >> 8) & 0xf) c.slices = (mode >> 8) & 0xf;
     if (over) {
         if (over->panel < 0 || over->panel > 2 || over->slices < 0 || over->slices > kSplitMaxSlices ||
-            over->ranges < 0 || over->ranges > 2 || over->epilogue < 0 || over->epilogue > 2)
+            over->ranges < 0 || over->ranges > 2 || over->epilogue < 0 || over->epilogue > 3)
             return false;
         if (over->panel) {
             if (over->panel == PFB_PANEL_HALF_SHARED && !hs_available(dtype, n)) return false;

@@ -172,6 +172,11 @@ PFB_D void mbar_arrive(uint32_t bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
+PFB_D void tmem_ld4(uint32_t taddr, int32_t (&v)[4])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "r"(taddr));
+}
 PFB_D void tmem_ld8(uint32_t taddr, int32_t (&v)[8])
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -679,6 +684,247 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
     }
 }
 
+// ------------------------------------------- transposed tiles, direct C access
+
+// Tiles of the transposed product for the direct epilogue: b-tile I covers 128
+// trailing columns (the MMA's M, TMEM lanes), a-tile J covers 64 trailing rows
+// (the MMA's N, TMEM columns); b-tile I meets the upper triangle in a-tiles
+// 0 .. 2I+1.  Walked backwards from the end of a CTA's range, like TileWalk.
+struct DirectWalk {
+    int nta, I, J;
+    PFB_D int count(int i) const { return 2 * i + 2 < nta ? 2 * i + 2 : nta; }
+    PFB_D void start(int idx)
+    {
+        I = 0;
+        while (idx >= count(I)) { idx -= count(I); I++; }
+        J = idx;
+    }
+    PFB_D void step()
+    {
+        if (--J < 0) { I--; J = count(I) - 1; }
+    }
+};
+
+// The split update with the tile transposed and the FP64 working matrix read
+// and written directly from global memory (real input; PFB_EPILOGUE_DIRECT).
+//
+// The MMA's A operand is the Y digits of 128 trailing columns b and its B
+// operand the X digits of 64 trailing rows a, so TMEM lane = column b and TMEM
+// column = row a: P_l[b][a] = sum_{i+j=l} Y_j[b] . X_i[a], the same integer
+// sums as split_update_kernel's (the products commute), hence the same bits.
+// An epilogue thread then owns one column b and 16 consecutive rows a, and the
+// 32 lanes of a warp own 32 adjacent columns: every load and store of C is a
+// coalesced 256-byte row segment.  The thread issues its 16 loads of C before
+// it waits for the accumulators (their latency hides behind the MMAs), folds
+// the S levels and adds them with one fused multiply-add per value, and
+// stores -- only the strictly upper part (a < b), the only part the
+// factorisation reads.  Shared memory holds operands only: the 128-column A
+// image (reused along a b-tile) and two 64-row B images, so the next tile's B
+// arrives while the current one multiplies.
+template <int KK, int S>
+__global__ void __maxnreg__(112)   // 576 threads: 65,536 / 576 registers, rounded down to 8
+split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, MatState *__restrict__ st_all,
+                           SplitArgs sa)
+{
+    constexpr int TM = kSplitTileM;             // b columns per tile (MMA M)
+    constexpr int TN = 64;                      // a rows per tile (MMA N)
+    constexpr uint32_t TMEM_COLS = 512;
+    static_assert(S * TN <= 448, "the S accumulators of a tile fit in TMEM");
+    extern __shared__ __align__(1024) unsigned char smem[];
+    constexpr int a_bytes = TM * KK;            // one slice of the A image (Y digits)
+    constexpr int b_bytes = TN * KK;            // one slice of one B image (X digits)
+    unsigned char *sA = smem;
+    unsigned char *sB = sA + kSplitMaxSlices * a_bytes;                    // two buffers
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + 2 * kSplitMaxSlices * b_bytes);
+    // bars: 0 a_full, 1 a_empty, 2-3 b_full, 4-5 b_empty, 6 acc_full, 7 acc_empty
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
+    int *s_fail = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int64_t b = blockIdx.y;
+    if (st_all[b].dead) return;
+    const int k1 = k0 + K;
+    const int m = n - k1;
+    const int ntb = (m + TM - 1) / TM;
+    const int nta = (m + TN - 1) / TN;
+    DirectWalk cw{nta, 0, 0};
+    int total = 0;
+    for (int I = 0; I < ntb; I++) total += cw.count(I);
+    const int t0 = (int)((int64_t)total * blockIdx.x / gridDim.x);
+    const int t1 = (int)((int64_t)total * (blockIdx.x + 1) / gridDim.x);
+    if (t0 >= t1) return;
+    const int ntiles = t1 - t0;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long lim = ((int)b == sa.fail_b) ? 0 : kWaitSpins;
+    const uint32_t bar0 = su32(bars);
+    auto mb = [bar0](int i) { return bar0 + 8u * (uint32_t)i; };
+    if (tid == 0) {
+        for (int i = 0; i < 8; i++) mbar_init(mb(i), i == 7 ? (uint32_t)kEpiThreads : 1u);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *s_fail = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(su32(tmem_slot)), "r"(TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    int p_aloads = 0, p_bloads = 0, m_issued = 0;
+    const int64_t chunk = (int64_t)TM * KK;
+
+    if (warp == 0) {
+        // ---------------- producer of the int8 operands
+        if (lane == 0) {
+            DirectWalk w{nta, 0, 0};
+            w.start(t1 - 1);
+            int brow = -1, aloads = 0;
+            for (int it = 0; it < ntiles && ok; it++, w.step()) {
+                if (w.I != brow) {
+                    if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1, lim);
+                    if (!ok) break;
+                    mbar_expect_tx(mb(0), (uint32_t)(S * a_bytes));
+                    for (int q = 0; q < S; q++)
+                        bulk_g2s(su32(sA + q * a_bytes), sa.ys + b * sa.mstride + ((int64_t)q * sa.ntile + w.I) * chunk,
+                                 a_bytes, mb(0));
+                    brow = w.I;
+                    aloads++;
+                    p_aloads = aloads;
+                }
+                const int bb = it & 1;
+                if (it >= 2) ok = mbar_wait_bounded(mb(4 + bb), ((it - 2) >> 1) & 1, lim);
+                if (!ok) break;
+                const int arow = w.J * TN;
+                const int64_t boff = (int64_t)(arow / TM) * chunk + (int64_t)((arow % TM) >> 3) * (KK >> 4) * 128;
+                mbar_expect_tx(mb(2 + bb), (uint32_t)(S * b_bytes));
+                for (int q = 0; q < S; q++)
+                    bulk_g2s(su32(sB + (bb * kSplitMaxSlices + q) * b_bytes),
+                             sa.xs + b * sa.mstride + (int64_t)q * sa.ntile * chunk + boff, b_bytes, mb(2 + bb));
+                p_bloads = it + 1;
+            }
+            if (!ok) atomicExch(s_fail, 1);
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_i8(TM, TN);
+            const uint32_t sbo = (uint32_t)(KK >> 4) * 128;
+            const uint64_t adesc0 = smem_desc(su32(sA), 128, sbo);
+            DirectWalk w{nta, 0, 0};
+            w.start(t1 - 1);
+            int brow = -1, aloads = 0;
+            for (int it = 0; it < ntiles && ok; it++, w.step()) {
+                if (w.I != brow) {
+                    if (aloads > 0) mma_commit(mb(1));
+                    ok = mbar_wait_bounded(mb(0), aloads & 1, lim);
+                    if (!ok) break;
+                    brow = w.I;
+                    aloads++;
+                }
+                const int bb = it & 1;
+                ok = mbar_wait_bounded(mb(2 + bb), (it >> 1) & 1, lim);
+                if (ok && it >= 1) ok = mbar_wait_bounded(mb(7), (it - 1) & 1, lim);
+                if (!ok) break;
+                tc_fence_after();
+                const uint64_t bdesc0 = smem_desc(su32(sB + bb * kSplitMaxSlices * b_bytes), 128, sbo);
+#pragma unroll
+                for (int l = 0; l < S; l++) {
+                    const uint32_t dcol = (uint32_t)(l * TN);
+#pragma unroll
+                    for (int i = 0; i <= l; i++) {
+                        // Y digit i of the columns with X digit l - i of the rows
+                        const uint64_t ad = adesc0 + (uint64_t)((i * a_bytes) >> 4);
+                        const uint64_t bd = bdesc0 + (uint64_t)(((l - i) * b_bytes) >> 4);
+#pragma unroll
+                        for (int kc = 0; kc < KK / 32; kc++)
+                            mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
+                                   (i > 0 || kc > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(mb(4 + bb));     // this B buffer is free once these MMAs are done
+                mma_commit(mb(6));          // accumulators ready
+                m_issued = it + 1;
+            }
+            if (!ok) atomicExch(s_fail, 1);
+        }
+    } else {
+        // ---------------- epilogue (warps 2-17): lane = column b, 16 rows a
+        const int quarter = warp & 3;
+        const int h = (warp - 2) >> 2;              // rows 16h .. 16h+15 of the a-tile
+        double *W = W_all + b * (int64_t)n * n;
+        DirectWalk w{nta, 0, 0};
+        w.start(t1 - 1);
+        for (int it = 0; it < ntiles && ok; it++, w.step()) {
+            const int col = k1 + w.I * TM + quarter * 32 + lane;     // this thread's column b
+            const int row0 = k1 + w.J * TN + 16 * h;                  // its first row a
+            const int eb = col < n ? __ldg(&sa.ex[b * n + col]) : 0;
+            const int ea_l = (lane < 16 && row0 + lane < n) ? __ldg(&sa.ex[b * n + row0 + lane]) : 0;
+            // C of this thread's 16 rows, loaded before the accumulators are waited for
+            double cv[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                const int a = row0 + c;
+                cv[c] = (a < col && col < n) ? W[(int64_t)a * n + col] : 0.0;
+            }
+            ok = epi_all(mbar_wait_bounded(mb(6), it & 1, lim));
+            if (!ok) break;
+            tc_fence_after();
+            // four rows at a time: S x 4 accumulator words in registers beside C
+#pragma unroll
+            for (int c4 = 0; c4 < 4; c4++) {
+                int32_t v[S][4];
+#pragma unroll
+                for (int l = 0; l < S; l++)
+                    tmem_ld4(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(l * TN + 16 * h + c4 * 4), v[l]);
+                tmem_ld_wait();
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    int32_t P[kSplitMaxSlices];
+#pragma unroll
+                    for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l < S ? l : 0][c] : 0;
+                    const double sc = exp2i(eb + __shfl_sync(0xffffffffu, ea_l, c4 * 4 + c) - 56);
+                    cv[c4 * 4 + c] = fma(fold_levels(P), sc, cv[c4 * 4 + c]);
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(mb(7));
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                const int a = row0 + c;
+                if (a < col && col < n) W[(int64_t)a * n + col] = cv[c];
+            }
+        }
+        if (!ok) atomicExch(s_fail, 1);
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (*s_fail) {
+        // a wait gave up: let this CTA's copies and MMAs in flight land (bounded) before exit
+        if (tid == 0) {
+            if (p_aloads > 0) mbar_wait_bounded(mb(0), (p_aloads - 1) & 1);
+            for (int t = (p_bloads > 2 ? p_bloads - 2 : 0); t < p_bloads; t++)
+                mbar_wait_bounded(mb(2 + (t & 1)), (t >> 1) & 1);
+            atomicExch(&sa.err[b], PFB_ERR_TIMEOUT);
+        }
+        if (tid == 32 && m_issued > 0) mbar_wait_bounded(mb(6), (m_issued - 1) & 1);
+        __syncthreads();
+    }
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+template <int KK>
+static size_t split_direct_smem_bytes()
+{
+    return (size_t)kSplitMaxSlices * kSplitTileM * KK + (size_t)2 * kSplitMaxSlices * 64 * KK + 8 * 8 + 16;
+}
+
 template <int TN, int NOUT, bool RED>
 static size_t split_smem_bytes(int kk)
 {
@@ -749,6 +995,30 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
+template <int KK, int S>
+static int launch_split_direct(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
+                               cudaStream_t stream)
+{
+    const int m = n - (k0 + K);
+    const int ntb = (m + kSplitTileM - 1) / kSplitTileM;
+    const int nta = (m + 63) / 64;
+    int tiles = 0;
+    for (int I = 0; I < ntb; I++) tiles += 2 * I + 2 < nta ? 2 * I + 2 : nta;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per = (int)(sms / batch);
+    if (per > (tiles + 1) / 2) per = (tiles + 1) / 2;
+    if (per < 1) per = 1;
+    auto k = split_update_direct_kernel<KK, S>;
+    const size_t smem = split_direct_smem_bytes<KK>();
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return PFB_ERR_CUDA;
+    k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(static_cast<double *>(W), n, k0, K, st,
+                                                                            sa);
+    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+}
+
 // one instantiation per (operand width, slices, epilogue): the MMA issue
 // unrolls; the reduce-add epilogue is built for 5 to 7 digits (the counts the
 // accuracy bar admits), fewer digits use the shared-memory round trip
@@ -757,6 +1027,16 @@ static int launch_split_s(void *W, int n, int k0, int K, int64_t batch, MatState
                           cudaStream_t stream)
 {
     const bool red = sa.epilogue == PFB_EPILOGUE_REDUCE;
+    if constexpr (NOUT == 1) {
+        if (sa.epilogue == PFB_EPILOGUE_DIRECT) {
+            switch (sa.slices) {
+            case 5: return launch_split_direct<KK, 5>(W, n, k0, K, batch, st, sa, stream);
+            case 6: return launch_split_direct<KK, 6>(W, n, k0, K, batch, st, sa, stream);
+            case 7: return launch_split_direct<KK, 7>(W, n, k0, K, batch, st, sa, stream);
+            default: break;   // fewer digits: the round trip below
+            }
+        }
+    }
     switch (sa.slices) {
     case 1: return launch_split_t<TN, NOUT, KK, 1, false>(W, n, k0, K, batch, st, sa, stream);
     case 2: return launch_split_t<TN, NOUT, KK, 2, false>(W, n, k0, K, batch, st, sa, stream);

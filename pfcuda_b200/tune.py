@@ -16,7 +16,8 @@ Knobs:
   ranges  1 | 2 (a batch of three or more waves of wide panel clusters split
           over two streams)
   epilogue  split update: roundtrip (C tile through shared memory) | reduce
-          (the increment added by the L2)
+          (the increment added by the L2) | direct (real: transposed tiles,
+          C read and written from global memory)
   slices  int8 digits per operand of the split update: 7 always qualifies; 6
           and 5 are kept only where the log error stays within
           --accuracy-margin x 1e-10 relative both on random matrices (against
@@ -143,7 +144,8 @@ def main():
                     ws = torch.empty(pf.slog_workspace_bytes(tdt, B, n, mode), dtype=torch.uint8, device="cuda")
                     panels = ["registers"] + (["half_shared"] if m2 > 0 else [])
                     slices = [7, 6, 5] if mode == "split" else [7]
-                    epis = ["roundtrip", "reduce"] if mode == "split" else ["roundtrip"]
+                    epis = ((["roundtrip", "reduce"] + ([] if cplx else ["direct"])) if mode == "split"
+                            else ["roundtrip"])
                     best = None
                     for panel in panels:
                         for ranges in (1, 2):

@@ -109,17 +109,20 @@ def test_config_overrides_are_checked():
 @pytest.mark.parametrize("cplx", [False, True])
 @pytest.mark.parametrize("n", [34, 66, 130, 256, 514, 1030])
 def test_split_epilogues_equal(cplx, n):
-    """The split update's two epilogues -- the C tile through shared memory
-    (round trip) and the L2 reduce-add of the increment -- round identically:
-    the increment value * 2^e is exact and C + increment is rounded once in
-    both, so results and pivots are equal bit for bit."""
+    """The split update's epilogues -- the C tile through shared memory (round
+    trip), the L2 reduce-add of the increment, and the transposed tile with C
+    read and written from global memory (direct; real input, complex falls
+    back to the round trip) -- round identically: the increment value * 2^e is
+    exact and C + increment is rounded once in each, so results and pivots
+    are equal bit for bit."""
     rng = np.random.default_rng(700 + n + cplx)
     A = O.skew_normal(rng, 3, n, scale=1 / np.sqrt(n), complex_=cplx)
     X = cuda(A)
     r1 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "roundtrip"})
     r2 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "reduce"})
-    for a, b in zip(r1, r2):
-        assert torch.equal(a, b)
+    r3 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "direct"})
+    for a, b, c in zip(r1, r2, r3):
+        assert torch.equal(a, b) and torch.equal(a, c)
     if n <= 256:
         wl, ws, wp = O.slog_pf(A, with_pivots=True)
         la, sg, piv = (x.cpu().numpy() for x in r2)
@@ -133,5 +136,7 @@ def test_split_epilogues_equal_at_the_headline_order():
     r1 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True, config={"epilogue": "roundtrip"})
     r2 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True,
                               config={"epilogue": "reduce", "panel": "half_shared"})
-    for a, b in zip(r1, r2):
-        assert torch.equal(a, b)
+    r3 = pf.slog_pfaffian_raw(X, mode="split", return_pivots=True,
+                              config={"epilogue": "direct", "panel": "half_shared"})
+    for a, b, c in zip(r1, r2, r3):
+        assert torch.equal(a, b) and torch.equal(a, c)
