@@ -687,12 +687,13 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
 // ------------------------------------------- transposed tiles, direct C access
 
 // Tiles of the transposed product for the direct epilogue: b-tile I covers 128
-// trailing columns (the MMA's M, TMEM lanes), a-tile J covers 64 trailing rows
-// (the MMA's N, TMEM columns); b-tile I meets the upper triangle in a-tiles
-// 0 .. 2I+1.  Walked backwards from the end of a CTA's range, like TileWalk.
+// trailing columns (the MMA's M, TMEM lanes), a-tile J covers TN trailing rows
+// (the MMA's N, TMEM columns; R = 128 / TN a-tiles per b-tile width); b-tile I
+// meets the upper triangle in a-tiles 0 .. (I+1) R - 1.  Walked backwards from
+// the end of a CTA's range, like TileWalk.
 struct DirectWalk {
-    int nta, I, J;
-    PFB_D int count(int i) const { return 2 * i + 2 < nta ? 2 * i + 2 : nta; }
+    int nta, R, I, J;
+    PFB_D int count(int i) const { return (i + 1) * R < nta ? (i + 1) * R : nta; }
     PFB_D void start(int idx)
     {
         I = 0;
@@ -705,36 +706,40 @@ struct DirectWalk {
     }
 };
 
-// The split update with the tile transposed and the FP64 working matrix read
-// and written directly from global memory (real input; PFB_EPILOGUE_DIRECT).
+// The split update with the tile transposed and the working matrix read and
+// written directly from global memory (PFB_EPILOGUE_DIRECT).
 //
 // The MMA's A operand is the Y digits of 128 trailing columns b and its B
-// operand the X digits of 64 trailing rows a, so TMEM lane = column b and TMEM
+// operand the X digits of TN trailing rows a, so TMEM lane = column b and TMEM
 // column = row a: P_l[b][a] = sum_{i+j=l} Y_j[b] . X_i[a], the same integer
 // sums as split_update_kernel's (the products commute), hence the same bits.
-// An epilogue thread then owns one column b and 16 consecutive rows a, and the
-// 32 lanes of a warp own 32 adjacent columns: every load and store of C is a
-// coalesced 256-byte row segment.  The thread issues its 16 loads of C before
-// it waits for the accumulators (their latency hides behind the MMAs), folds
-// the S levels and adds them with one fused multiply-add per value, and
-// stores -- only the strictly upper part (a < b), the only part the
-// factorisation reads.  Shared memory holds operands only: the 128-column A
-// image (reused along a b-tile) and two 64-row B images, so the next tile's B
-// arrives while the current one multiplies.
-template <int KK, int S>
+// Complex input (NOUT = 2, TN = 32 complex rows) multiplies two A images --
+// [Yr | -Yi] for the real part and [Yi | Yr] for the imaginary part -- by one B
+// image [Xr | Xi].  An epilogue thread owns one column b and TN / 4
+// consecutive rows a, and the 32 lanes of a warp own 32 adjacent columns:
+// every load and store of C is a coalesced row segment (256 bytes real, 512
+// complex).  The thread issues its loads of C before it waits for the
+// accumulators (their latency hides behind the MMAs), reads the S levels from
+// TMEM four rows at a time, folds them and adds them with one fused
+// multiply-add per value, and stores only the strictly upper part (a < b), the
+// only part the factorisation reads.  Shared memory holds operands only: the A
+// image(s) of a b-tile (reused along it) and two B images, so the next tile's
+// B arrives while the current one multiplies.
+template <int NOUT, int KK, int S>
 __global__ void __maxnreg__(112)   // 576 threads: 65,536 / 576 registers, rounded down to 8
 split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, MatState *__restrict__ st_all,
                            SplitArgs sa)
 {
     constexpr int TM = kSplitTileM;             // b columns per tile (MMA M)
-    constexpr int TN = 64;                      // a rows per tile (MMA N)
+    constexpr int TN = 64 / NOUT;               // a rows per tile (MMA N)
+    constexpr int RW = TN / 4;                  // rows per epilogue thread
     constexpr uint32_t TMEM_COLS = 512;
-    static_assert(S * TN <= 448, "the S accumulators of a tile fit in TMEM");
+    static_assert(NOUT * S * TN <= 448, "the S accumulators of a tile fit in TMEM");
     extern __shared__ __align__(1024) unsigned char smem[];
-    constexpr int a_bytes = TM * KK;            // one slice of the A image (Y digits)
+    constexpr int a_bytes = TM * KK;            // one slice of one A image (Y digits)
     constexpr int b_bytes = TN * KK;            // one slice of one B image (X digits)
-    unsigned char *sA = smem;
-    unsigned char *sB = sA + kSplitMaxSlices * a_bytes;                    // two buffers
+    unsigned char *sA = smem;                                              // NOUT images
+    unsigned char *sB = sA + NOUT * kSplitMaxSlices * a_bytes;             // two buffers
     uint64_t *bars = reinterpret_cast<uint64_t *>(sB + 2 * kSplitMaxSlices * b_bytes);
     // bars: 0 a_full, 1 a_empty, 2-3 b_full, 4-5 b_empty, 6 acc_full, 7 acc_empty
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
@@ -746,7 +751,8 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
     const int m = n - k1;
     const int ntb = (m + TM - 1) / TM;
     const int nta = (m + TN - 1) / TN;
-    DirectWalk cw{nta, 0, 0};
+    constexpr int R = TM / TN;
+    DirectWalk cw{nta, R, 0, 0};
     int total = 0;
     for (int I = 0; I < ntb; I++) total += cw.count(I);
     const int t0 = (int)((int64_t)total * blockIdx.x / gridDim.x);
@@ -779,17 +785,20 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
     if (warp == 0) {
         // ---------------- producer of the int8 operands
         if (lane == 0) {
-            DirectWalk w{nta, 0, 0};
+            DirectWalk w{nta, R, 0, 0};
             w.start(t1 - 1);
             int brow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, w.step()) {
                 if (w.I != brow) {
                     if (aloads > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1, lim);
                     if (!ok) break;
-                    mbar_expect_tx(mb(0), (uint32_t)(S * a_bytes));
-                    for (int q = 0; q < S; q++)
-                        bulk_g2s(su32(sA + q * a_bytes), sa.ys + b * sa.mstride + ((int64_t)q * sa.ntile + w.I) * chunk,
-                                 a_bytes, mb(0));
+                    mbar_expect_tx(mb(0), (uint32_t)(NOUT * S * a_bytes));
+                    for (int o = 0; o < NOUT; o++)
+                        for (int q = 0; q < S; q++)
+                            bulk_g2s(su32(sA + (o * kSplitMaxSlices + q) * a_bytes),
+                                     (o == 0 ? sa.ys : sa.ys2) + b * sa.mstride +
+                                         ((int64_t)q * sa.ntile + w.I) * chunk,
+                                     a_bytes, mb(0));
                     brow = w.I;
                     aloads++;
                     p_aloads = aloads;
@@ -813,7 +822,7 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
             constexpr uint32_t idesc = idesc_i8(TM, TN);
             const uint32_t sbo = (uint32_t)(KK >> 4) * 128;
             const uint64_t adesc0 = smem_desc(su32(sA), 128, sbo);
-            DirectWalk w{nta, 0, 0};
+            DirectWalk w{nta, R, 0, 0};
             w.start(t1 - 1);
             int brow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, w.step()) {
@@ -831,17 +840,20 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
                 tc_fence_after();
                 const uint64_t bdesc0 = smem_desc(su32(sB + bb * kSplitMaxSlices * b_bytes), 128, sbo);
 #pragma unroll
-                for (int l = 0; l < S; l++) {
-                    const uint32_t dcol = (uint32_t)(l * TN);
+                for (int o = 0; o < NOUT; o++) {
 #pragma unroll
-                    for (int i = 0; i <= l; i++) {
-                        // Y digit i of the columns with X digit l - i of the rows
-                        const uint64_t ad = adesc0 + (uint64_t)((i * a_bytes) >> 4);
-                        const uint64_t bd = bdesc0 + (uint64_t)(((l - i) * b_bytes) >> 4);
+                    for (int l = 0; l < S; l++) {
+                        const uint32_t dcol = (uint32_t)((o * S + l) * TN);
 #pragma unroll
-                        for (int kc = 0; kc < KK / 32; kc++)
-                            mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
-                                   (i > 0 || kc > 0) ? 1u : 0u);
+                        for (int i = 0; i <= l; i++) {
+                            // Y digit i of the columns with X digit l - i of the rows
+                            const uint64_t ad = adesc0 + (uint64_t)(((o * kSplitMaxSlices + i) * a_bytes) >> 4);
+                            const uint64_t bd = bdesc0 + (uint64_t)(((l - i) * b_bytes) >> 4);
+#pragma unroll
+                            for (int kc = 0; kc < KK / 32; kc++)
+                                mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
+                                       (i > 0 || kc > 0) ? 1u : 0u);
+                        }
                     }
                 }
                 mma_commit(mb(4 + bb));     // this B buffer is free once these MMAs are done
@@ -851,50 +863,66 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
             if (!ok) atomicExch(s_fail, 1);
         }
     } else {
-        // ---------------- epilogue (warps 2-17): lane = column b, 16 rows a
+        // ---------------- epilogue (warps 2-17): lane = column b, RW rows a
         const int quarter = warp & 3;
-        const int h = (warp - 2) >> 2;              // rows 16h .. 16h+15 of the a-tile
-        double *W = W_all + b * (int64_t)n * n;
-        DirectWalk w{nta, 0, 0};
+        const int h = (warp - 2) >> 2;              // rows RW h .. RW h + RW - 1 of the a-tile
+        double *W = W_all + b * (int64_t)NOUT * n * n;
+        DirectWalk w{nta, R, 0, 0};
         w.start(t1 - 1);
         for (int it = 0; it < ntiles && ok; it++, w.step()) {
             const int col = k1 + w.I * TM + quarter * 32 + lane;     // this thread's column b
-            const int row0 = k1 + w.J * TN + 16 * h;                  // its first row a
+            const int row0 = k1 + w.J * TN + RW * h;                  // its first row a
             const int eb = col < n ? __ldg(&sa.ex[b * n + col]) : 0;
-            const int ea_l = (lane < 16 && row0 + lane < n) ? __ldg(&sa.ex[b * n + row0 + lane]) : 0;
-            // C of this thread's 16 rows, loaded before the accumulators are waited for
-            double cv[16];
+            const int ea_l = (lane < RW && row0 + lane < n) ? __ldg(&sa.ex[b * n + row0 + lane]) : 0;
+            // C of this thread's rows, loaded before the accumulators are waited for
+            double cv[RW][NOUT];
 #pragma unroll
-            for (int c = 0; c < 16; c++) {
+            for (int c = 0; c < RW; c++) {
                 const int a = row0 + c;
-                cv[c] = (a < col && col < n) ? W[(int64_t)a * n + col] : 0.0;
+                const bool up = a < col && col < n;
+                const int64_t e = ((int64_t)a * n + col) * NOUT;
+                if constexpr (NOUT == 1) {
+                    cv[c][0] = up ? W[e] : 0.0;
+                } else {
+                    const double2 z = up ? *reinterpret_cast<const double2 *>(W + e) : make_double2(0.0, 0.0);
+                    cv[c][0] = z.x;
+                    cv[c][NOUT - 1] = z.y;
+                }
             }
             ok = epi_all(mbar_wait_bounded(mb(6), it & 1, lim));
             if (!ok) break;
             tc_fence_after();
-            // four rows at a time: S x 4 accumulator words in registers beside C
+            // four rows at a time: S x 4 accumulator words per output beside C
 #pragma unroll
-            for (int c4 = 0; c4 < 4; c4++) {
-                int32_t v[S][4];
+            for (int c4 = 0; c4 < RW / 4; c4++) {
 #pragma unroll
-                for (int l = 0; l < S; l++)
-                    tmem_ld4(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(l * TN + 16 * h + c4 * 4), v[l]);
-                tmem_ld_wait();
+                for (int o = 0; o < NOUT; o++) {
+                    int32_t v[S][4];
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    int32_t P[kSplitMaxSlices];
+                    for (int l = 0; l < S; l++)
+                        tmem_ld4(tmem + ((uint32_t)(quarter * 32) << 16) +
+                                     (uint32_t)((o * S + l) * TN + RW * h + c4 * 4), v[l]);
+                    tmem_ld_wait();
 #pragma unroll
-                    for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l < S ? l : 0][c] : 0;
-                    const double sc = exp2i(eb + __shfl_sync(0xffffffffu, ea_l, c4 * 4 + c) - 56);
-                    cv[c4 * 4 + c] = fma(fold_levels(P), sc, cv[c4 * 4 + c]);
+                    for (int c = 0; c < 4; c++) {
+                        int32_t P[kSplitMaxSlices];
+#pragma unroll
+                        for (int l = 0; l < kSplitMaxSlices; l++) P[l] = l < S ? v[l < S ? l : 0][c] : 0;
+                        const double sc = exp2i(eb + __shfl_sync(0xffffffffu, ea_l, c4 * 4 + c) - 56);
+                        cv[c4 * 4 + c][o] = fma(fold_levels(P), sc, cv[c4 * 4 + c][o]);
+                    }
                 }
             }
             tc_fence_before();
             mbar_arrive(mb(7));
 #pragma unroll
-            for (int c = 0; c < 16; c++) {
+            for (int c = 0; c < RW; c++) {
                 const int a = row0 + c;
-                if (a < col && col < n) W[(int64_t)a * n + col] = cv[c];
+                if (a < col && col < n) {
+                    const int64_t e = ((int64_t)a * n + col) * NOUT;
+                    if constexpr (NOUT == 1) W[e] = cv[c][0];
+                    else *reinterpret_cast<double2 *>(W + e) = make_double2(cv[c][0], cv[c][NOUT - 1]);
+                }
             }
         }
         if (!ok) atomicExch(s_fail, 1);
@@ -919,10 +947,11 @@ split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, Mat
     }
 }
 
-template <int KK>
+template <int NOUT, int KK>
 static size_t split_direct_smem_bytes()
 {
-    return (size_t)kSplitMaxSlices * kSplitTileM * KK + (size_t)2 * kSplitMaxSlices * 64 * KK + 8 * 8 + 16;
+    return (size_t)NOUT * kSplitMaxSlices * kSplitTileM * KK + (size_t)2 * kSplitMaxSlices * (64 / NOUT) * KK +
+           8 * 8 + 16;
 }
 
 template <int TN, int NOUT, bool RED>
@@ -995,23 +1024,24 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
 }
 
-template <int KK, int S>
+template <int NOUT, int KK, int S>
 static int launch_split_direct(void *W, int n, int k0, int K, int64_t batch, MatState *st, const SplitArgs &sa,
                                cudaStream_t stream)
 {
+    constexpr int TN = 64 / NOUT, R = kSplitTileM / TN;
     const int m = n - (k0 + K);
     const int ntb = (m + kSplitTileM - 1) / kSplitTileM;
-    const int nta = (m + 63) / 64;
+    const int nta = (m + TN - 1) / TN;
     int tiles = 0;
-    for (int I = 0; I < ntb; I++) tiles += 2 * I + 2 < nta ? 2 * I + 2 : nta;
+    for (int I = 0; I < ntb; I++) tiles += (I + 1) * R < nta ? (I + 1) * R : nta;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int per = (int)(sms / batch);
     if (per > (tiles + 1) / 2) per = (tiles + 1) / 2;
     if (per < 1) per = 1;
-    auto k = split_update_direct_kernel<KK, S>;
-    const size_t smem = split_direct_smem_bytes<KK>();
+    auto k = split_update_direct_kernel<NOUT, KK, S>;
+    const size_t smem = split_direct_smem_bytes<NOUT, KK>();
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PFB_ERR_CUDA;
     k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(static_cast<double *>(W), n, k0, K, st,
@@ -1027,14 +1057,12 @@ static int launch_split_s(void *W, int n, int k0, int K, int64_t batch, MatState
                           cudaStream_t stream)
 {
     const bool red = sa.epilogue == PFB_EPILOGUE_REDUCE;
-    if constexpr (NOUT == 1) {
-        if (sa.epilogue == PFB_EPILOGUE_DIRECT) {
-            switch (sa.slices) {
-            case 5: return launch_split_direct<KK, 5>(W, n, k0, K, batch, st, sa, stream);
-            case 6: return launch_split_direct<KK, 6>(W, n, k0, K, batch, st, sa, stream);
-            case 7: return launch_split_direct<KK, 7>(W, n, k0, K, batch, st, sa, stream);
-            default: break;   // fewer digits: the round trip below
-            }
+    if (sa.epilogue == PFB_EPILOGUE_DIRECT) {
+        switch (sa.slices) {
+        case 5: return launch_split_direct<NOUT, KK, 5>(W, n, k0, K, batch, st, sa, stream);
+        case 6: return launch_split_direct<NOUT, KK, 6>(W, n, k0, K, batch, st, sa, stream);
+        case 7: return launch_split_direct<NOUT, KK, 7>(W, n, k0, K, batch, st, sa, stream);
+        default: break;   // fewer digits: the round trip below
         }
     }
     switch (sa.slices) {
