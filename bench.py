@@ -463,9 +463,14 @@ def wl_illcond(torch, pf, _lib, O, dev, stream, steps, warmup):
                                 np.linalg.norm(Y.reshape(2, -1), axis=1)))
 
         if npdt == np.float64:
-            # the exact adjoint of the construction; bar cond * sqrt(n) * eps * 4
+            # the exact adjoint of the construction; bar 4 cond sqrt(n) u with u
+            # the unit of the split update (sqrt(K) 2^(-7S), K = 64, S = 7); the
+            # FP64 path's adjoint, with u = eps, beside it
             r["vjp_max_rel_frobenius_err_vs_exact"] = frob(G, G_exact)
-            r["vjp_bar"] = 1e6 * np.sqrt(n) * np.finfo(np.float64).eps * 4
+            r["vjp_bar"] = 4 * 1e6 * np.sqrt(n) * np.sqrt(64) * 2.0 ** -49
+            G64 = pf.slog_pfaffian_grad(A[:2], mode="fp64").cpu().numpy()
+            r["vjp_fp64_max_rel_frobenius_err_vs_exact"] = frob(G64, G_exact)
+            r["vjp_fp64_bar"] = 4 * 1e6 * np.sqrt(n) * np.finfo(np.float64).eps
         else:
             # the float32 matrices are the float64 ones rounded (cond 1e6), so the
             # exact adjoint is out of reach; compared with NumPy's FP64 inverse of
