@@ -11,10 +11,14 @@
 namespace {
 thread_local int g_last_cuda_error = 0;
 
-int cuda_status(cudaError_t e)
+int cuda_status(cudaError_t e) { return pfb::cuda_check(e); }
+
+// A call that failed with PFB_ERR_CUDA recorded its error where it happened; a
+// runtime error still pending (a failed attribute call, say) is recorded too.
+int cuda_failed()
 {
-    if (e == cudaSuccess) return PFB_OK;
-    g_last_cuda_error = (int)e;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) g_last_cuda_error = (int)e;
     return PFB_ERR_CUDA;
 }
 
@@ -25,6 +29,10 @@ size_t dtype_bytes(int d) { return d == PFB_F32 ? 4 : (d == PFB_C128 ? 16 : 8); 
 
 constexpr int kUploadRows = 256;   // rows per rectangle of pfb_upload_upper
 }  // namespace
+
+namespace pfb {
+int &last_cuda_error() { return g_last_cuda_error; }
+}
 
 extern "C" {
 
@@ -52,7 +60,7 @@ int pfb_pfaffian(int dtype, const void *A, int64_t batch, int n, int layout, voi
     if (!out || (!A && n > 0)) return PFB_ERR_INVALID;
     int rc = pfb::launch_small(dtype, false, A, batch, n, layout, out, nullptr, nullptr,
                                (cudaStream_t)stream);
-    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    if (rc == PFB_ERR_CUDA) return cuda_failed();
     return rc;
 }
 
@@ -135,7 +143,7 @@ int pfb_slog_pfaffian_ex(int dtype, const void *A, int64_t batch, int n, int lay
         rc = pfb::launch_large(dtype, A, batch, n, layout, mode, log_out, sign_out, workspace,
                                workspace_bytes, s, timing, config);
     }
-    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    if (rc == PFB_ERR_CUDA) return cuda_failed();
     return rc;
 }
 
@@ -153,7 +161,7 @@ int pfb_slog_pfaffian_ptrs(int dtype, const void *const *A_ptrs, int64_t batch, 
     if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
     const int rc = pfb::launch_large(dtype, nullptr, batch, n, layout, mode, log_out, sign_out, workspace,
                                      workspace_bytes, (cudaStream_t)stream, nullptr, nullptr, A_ptrs);
-    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    if (rc == PFB_ERR_CUDA) return cuda_failed();
     return rc;
 }
 
@@ -178,7 +186,7 @@ int pfb_slog_pfaffian_grad(int dtype, const void *A, int64_t batch, int n, int l
     if (!workspace || workspace_bytes < need1 || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
     const int rc = pfb::launch_grad(dtype, A, batch, n, layout, mode, ct_log, G_out, log_out, sign_out,
                                     workspace, workspace_bytes, (cudaStream_t)stream);
-    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    if (rc == PFB_ERR_CUDA) return cuda_failed();
     return rc;
 }
 
@@ -199,7 +207,7 @@ int pfb_slog_pfaffian_ragged(const void *const *A, const int32_t *n, const int32
     if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255u)) return PFB_ERR_WORKSPACE;
     const int rc = pfb::launch_ragged(A, n, dtype, count, max_n, layout, log_out, sign_out, workspace,
                                       (cudaStream_t)stream);
-    if (rc == PFB_ERR_CUDA) return cuda_status(cudaGetLastError());
+    if (rc == PFB_ERR_CUDA) return cuda_failed();
     return rc;
 }
 

@@ -144,6 +144,21 @@ PFB_D c128 ldg(const c128 *p)
     return mk(v.x, v.y);
 }
 
+// The CUDA error of the calling host thread's most recent failing call (what
+// pfb_last_cuda_error returns); defined in capi.cu.
+int &last_cuda_error();
+
+// PFB_OK, or PFB_ERR_CUDA with the error recorded, for a runtime call's result.
+inline int cuda_check(cudaError_t e)
+{
+    if (e == cudaSuccess) return PFB_OK;
+    last_cuda_error() = (int)e;
+    return PFB_ERR_CUDA;
+}
+// The same for the launches just made (cudaGetLastError clears a launch error,
+// so it is recorded here, where it is read).
+inline int launch_status() { return cuda_check(cudaGetLastError()); }
+
 // dtype enum -> storage type
 template <int D> struct DT;
 template <> struct DT<PFB_F32> { using type = float; };

@@ -352,15 +352,13 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
     {
         auto k = grad_diag_inv_kernel<T>;
         const size_t sm = 2 * kGB * kGB * sizeof(T);
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-            return PFB_ERR_CUDA;
+        if (cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != PFB_OK) return PFB_ERR_CUDA;
         k<<<dim3((unsigned)nblk, ub), kGB, sm, s>>>(W, Y, V.st, n);
     }
     {
         auto k = grad_block_row_kernel<T>;
         const size_t sm = block_row_smem<T>();
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-            return PFB_ERR_CUDA;
+        if (cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != PFB_OK) return PFB_ERR_CUDA;
         for (int I = nblk - 2; I >= 0; I--) {
             const int r0 = I * kGB;
             const int tiles = (n - (r0 + kGB) + kGB - 1) / kGB;
@@ -388,7 +386,7 @@ static int run_grad(int dtype, const void *A, int64_t B, int n, int layout, int 
             k<<<dim3(tiles, ub), 256, sm, s>>>((const c128 *)W, (const c128 *)Y, perm, V.st, ct, n, (c128 *)G);
         }
     }
-    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+    return launch_status();
 }
 
 // The largest number of matrices (<= batch) whose adjoint fits in `bytes` of

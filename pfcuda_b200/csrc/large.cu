@@ -388,7 +388,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
             copy_in_kernel<c128, c128><<<(unsigned)blocks, 256, 0, s>>>((const c128 *)A, (const c128 *const *)Ap, (c128 *)W, B, n, st);
             break;
         }
-        if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
+        if (launch_status() != PFB_OK) return PFB_ERR_CUDA;
     }
 
     // the panel form: the whole window in registers (one CTA per SM), or half
@@ -401,10 +401,8 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
             psmem = sizeof(PanelSmemHS<T, NB>);
         }
     }
-    if (cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) != cudaSuccess)
-        return PFB_ERR_CUDA;
-    if (cudaFuncSetAttribute(pk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-        return PFB_ERR_CUDA;
+    if (cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem)) != PFB_OK) return PFB_ERR_CUDA;
+    if (cuda_check(cudaFuncSetAttribute(pk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != PFB_OK) return PFB_ERR_CUDA;
 
     constexpr bool cplx = IsComplex<T>::value;
     // FP64 tensor-core tiles: 128 x 128 real, 64 x 64 complex
@@ -418,8 +416,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
         gk = (void *)gemm_dmma_kernel<NB>;
         gsmem = (size_t)2 * NB * kDmmaLD * sizeof(double);
     }
-    if (cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem) != cudaSuccess)
-        return PFB_ERR_CUDA;
+    if (cuda_check(cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem)) != PFB_OK) return PFB_ERR_CUDA;
 
     SplitArgs sa{};
     unsigned char *split_ws = ws + L.split_off;
@@ -427,7 +424,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
     int32_t *split_err = nullptr;
     if ((mode & 0xff) == PFB_MODE_SPLIT) {
         split_err = split_args(true, split_ws, cplx, batch, n, NB, 0, slices).err + b0;
-        if (cudaMemsetAsync(split_err, 0, (size_t)B * sizeof(int32_t), s) != cudaSuccess) return PFB_ERR_CUDA;
+        if (cuda_check(cudaMemsetAsync(split_err, 0, (size_t)B * sizeof(int32_t), s)) != PFB_OK) return PFB_ERR_CUDA;
     }
     auto rec = [&](void **evs, int i) {
         if (tm && evs && i < 2 * tm->pairs) cudaEventRecord((cudaEvent_t)evs[i], s);
@@ -458,7 +455,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         rec(tm ? tm->panel_events : nullptr, 2 * panel_idx);
-        if (cudaLaunchKernelEx(&cfg, pk, W, n, k0, st, piv) != cudaSuccess) return PFB_ERR_CUDA;
+        if (cuda_check(cudaLaunchKernelEx(&cfg, pk, W, n, k0, st, piv)) != PFB_OK) return PFB_ERR_CUDA;
         rec(tm ? tm->panel_events : nullptr, 2 * panel_idx + 1);
 
         if (mt > 0) {
@@ -467,7 +464,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
                 constexpr int cpb = 256 / (NB / 16);
                 split_slice_kernel<T, NB><<<dim3((unsigned)((mt + cpb - 1) / cpb), (unsigned)B), 256, 0, s>>>(
                     W, n, k0, st, sa);
-                if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
+                if (launch_status() != PFB_OK) return PFB_ERR_CUDA;
                 int rc = launch_split_update(cplx, W, n, k0, K, B, st, sa, s);
                 if (rc != PFB_OK) return rc;
             } else {
@@ -480,7 +477,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
                     gemm_zdmma_kernel<NB><<<dim3((unsigned)B, tiles), 256, gsmem, s>>>(W, n, k0, K, st);
                 else
                     gemm_dmma_kernel<NB><<<dim3((unsigned)B, tiles), kDmmaThreads, gsmem, s>>>(W, n, k0, K, st);
-                if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
+                if (launch_status() != PFB_OK) return PFB_ERR_CUDA;
             }
             rec(tm ? tm->update_events : nullptr, 2 * panel_idx + 1);
         }
@@ -494,7 +491,7 @@ static int run_large(const void *A, const void *const *Ap, int dtype, int64_t ba
     case PFB_C64: finalize_kernel<c64><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (c64 *)sign_out); break;
     default: finalize_kernel<c128><<<fb, 128, 0, s>>>(st, split_err, B, negate, log_out, (c128 *)sign_out); break;
     }
-    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NB, int CPT>

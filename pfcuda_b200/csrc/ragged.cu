@@ -314,7 +314,7 @@ int launch_ragged(const void *const *A, const int32_t *n, const int32_t *dtype, 
     unsigned char *ws = static_cast<unsigned char *>(workspace);
     ragged_order_kernel<<<1, 1024, 0, s>>>(n, count, reinterpret_cast<int32_t *>(ws + L.order_off),
                                           reinterpret_cast<int *>(ws + L.counter_off));
-    if (cudaGetLastError() != cudaSuccess) return PFB_ERR_CUDA;
+    if (launch_status() != PFB_OK) return PFB_ERR_CUDA;
     if (max_n <= RaggedCfg<16>::kMaxN)
         return launch_ragged_nb<16>(A, n, dtype, count, max_n, layout, log_out, sign_out, ws, L, s);
     return launch_ragged_nb<32>(A, n, dtype, count, max_n, layout, log_out, sign_out, ws, L, s);

@@ -238,7 +238,7 @@ static int launch_small_t(const void *A, int64_t batch, int n, int layout, void 
         pf_small_kernel<T, 16, SLOG><<<grid, block, 0, stream>>>(a, batch, n, flip, ov, out_log, os);
     else
         pf_small_kernel<T, 32, SLOG><<<grid, block, 0, stream>>>(a, batch, n, flip, ov, out_log, os);
-    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_small(int dtype, bool slog, const void *A, int64_t batch, int n, int layout,

@@ -726,7 +726,7 @@ struct DirectWalk {
 // image(s) of a b-tile (reused along it) and two B images, so the next tile's
 // B arrives while the current one multiplies.
 template <int NOUT, int KK, int S>
-__global__ void __maxnreg__(112)   // 576 threads: 65,536 / 576 registers, rounded down to 8
+__global__ void __launch_bounds__(kSplitThreads, 1)   // 96 registers: 5 of the 18 warps share an SM partition
 split_update_direct_kernel(double *__restrict__ W_all, int n, int k0, int K, MatState *__restrict__ st_all,
                            SplitArgs sa)
 {
@@ -1017,11 +1017,10 @@ static int launch_split_t(void *W, int n, int k0, int K, int64_t batch, MatState
     if (!RED && !make_c_map(&map, W, n, NOUT, batch)) return PFB_ERR_UNSUPPORTED;
     auto k = split_update_kernel<TN, NOUT, KK, S, RED>;
     const size_t smem = split_smem_bytes<TN, NOUT, RED>(KK);
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return PFB_ERR_CUDA;
+    if (cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != PFB_OK) return PFB_ERR_CUDA;
     k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(map, static_cast<double *>(W), n,
                                                                             k0, K, st, sa);
-    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+    return launch_status();
 }
 
 template <int NOUT, int KK, int S>
@@ -1042,11 +1041,10 @@ static int launch_split_direct(void *W, int n, int k0, int K, int64_t batch, Mat
     if (per < 1) per = 1;
     auto k = split_update_direct_kernel<NOUT, KK, S>;
     const size_t smem = split_direct_smem_bytes<NOUT, KK>();
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return PFB_ERR_CUDA;
+    if (cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != PFB_OK) return PFB_ERR_CUDA;
     k<<<dim3((unsigned)per, (unsigned)batch), kSplitThreads, smem, stream>>>(static_cast<double *>(W), n, k0, K, st,
                                                                             sa);
-    return cudaGetLastError() == cudaSuccess ? PFB_OK : PFB_ERR_CUDA;
+    return launch_status();
 }
 
 // one instantiation per (operand width, slices, epilogue): the MMA issue
