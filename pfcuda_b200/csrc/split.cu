@@ -38,12 +38,12 @@
 
 #include "split.cuh"
 #include "large.cuh"
+#include "tma.cuh"
 
 namespace pfb {
 
 constexpr int kSplitThreads = 576;   // warp 0: loads, warp 1: MMA, warps 2-17: epilogue
 constexpr int kEpiThreads = 512;
-constexpr long long kWaitSpins = 1LL << 24;   // bounded mbarrier polling
 
 bool split_available()
 {
@@ -91,31 +91,6 @@ SplitArgs split_args(bool use, unsigned char *ws, bool cplx, int64_t batch, int 
 
 // ------------------------------------------------------------- PTX wrappers
 
-PFB_D uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-PFB_D void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-PFB_D void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-PFB_D bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
-    return ok != 0;
-}
-PFB_D bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit = kWaitSpins)
-{
-    for (long long i = 0; i < limit; i++)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
 PFB_D void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -205,12 +180,6 @@ struct TileWalk {
 
 // ------------------------------------------------- tensor-map (TMA) helpers
 
-PFB_D void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%2, %3, %4}], [%5];"
-                 ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
-}
 PFB_D void tma_store_3d(const CUtensorMap *map, int x, int y, int z, uint32_t src)
 {
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
@@ -959,26 +928,6 @@ static size_t split_smem_bytes(int kk)
 {
     return (size_t)2 * (RED ? kDeltaTileBytes : kCTileBytes) + (size_t)kSplitMaxSlices * kSplitTileM * kk +
            (size_t)NOUT * kSplitMaxSlices * TN * kk + 8 * 8 + 16;
-}
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// against libcuda).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_tiled()
-{
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
 }
 
 // W of a batch as a 3-D FP64 tensor {NOUT*n columns, n rows, batch}, boxes of
