@@ -125,6 +125,22 @@ PFB_D void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t ides
                  "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
                  ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
 }
+// The same product with A (128 rows x 32 int8 per lane: K packed four to a
+// column) in tensor memory at column address tmem_a.
+PFB_D void mma_i8_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}"
+                 ::"r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+// 128 rows x 32 bytes of a K-major operand in shared memory (descriptor sdesc)
+// into 128 lanes x 8 columns of tensor memory at taddr, ordered with the
+// issuing thread's later MMAs.
+PFB_D void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc)
+{
+    asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(taddr), "l"(sdesc) : "memory");
+}
 PFB_D void mma_commit(uint32_t bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -305,6 +321,12 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
     constexpr int CW = TN / 4;                  // logical columns per epilogue thread
     static_assert(TN * NOUT == 64, "a C tile is 64 doubles wide");
     static_assert(NOUT * S * TN <= 448, "the S accumulators of a tile fit in TMEM");
+    // The A digits of slices 0 .. kTmemA-1 live in tensor memory after the
+    // accumulators (K/4 columns a slice), so their MMAs read only B from shared
+    // memory: an int8 MMA of 128 x 64 x 32 reading both operands from shared
+    // memory (6 KB) is bound by its bandwidth, not by the tensor pipe.
+    constexpr int kAcol0 = NOUT * S * TN;
+    constexpr int kTmemA = (512 - kAcol0) / (KK / 4) < S ? (512 - kAcol0) / (KK / 4) : S;
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr int kk = KK;
     constexpr int a_bytes = TM * kk;            // one slice of the A tile
@@ -406,9 +428,21 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             int arow = -1, aloads = 0;
             for (int it = 0; it < ntiles && ok; it++, tw.step()) {
                 if (tw.I != arow) {
-                    if (aloads > 0) mma_commit(mb(1));          // A may be replaced once these MMAs finish
+                    if (aloads > 0) {
+                        mma_commit(mb(1));          // A may be replaced once these MMAs finish
+                        // and the tensor-memory image of A is rewritten below
+                        if (kTmemA > 0) ok = mbar_wait_bounded(mb(1), (aloads - 1) & 1, lim);
+                        if (!ok) break;
+                    }
                     ok = mbar_wait_bounded(mb(0), aloads & 1, lim);
                     if (!ok) break;
+                    tc_fence_after();
+#pragma unroll
+                    for (int i = 0; i < kTmemA; i++)
+#pragma unroll
+                        for (int kc = 0; kc < kk / 32; kc++)
+                            tmem_cp_128x256b(tmem + kAcol0 + (uint32_t)(i * (kk / 4) + kc * 8),
+                                             adesc0 + (uint64_t)(((i * a_bytes) >> 4) + kc * 16));
                     arow = tw.I;
                     aloads++;
                 }
@@ -426,9 +460,14 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
                             const uint64_t ad = adesc0 + (uint64_t)((i * a_bytes) >> 4);
                             const uint64_t bd = bdesc0 + (uint64_t)(((o * kSplitMaxSlices + (l - i)) * b_bytes) >> 4);
 #pragma unroll
-                            for (int kc = 0; kc < kk / 32; kc++)
-                                mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
-                                       (i > 0 || kc > 0) ? 1u : 0u);
+                            for (int kc = 0; kc < kk / 32; kc++) {
+                                if (i < kTmemA)
+                                    mma_i8_ts(tmem + dcol, tmem + kAcol0 + (uint32_t)(i * (kk / 4) + kc * 8),
+                                              bd + (uint64_t)(kc * 16), idesc, (i > 0 || kc > 0) ? 1u : 0u);
+                                else
+                                    mma_i8(tmem + dcol, ad + (uint64_t)(kc * 16), bd + (uint64_t)(kc * 16), idesc,
+                                           (i > 0 || kc > 0) ? 1u : 0u);
+                            }
                         }
                     }
                 }
