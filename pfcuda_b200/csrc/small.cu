@@ -41,6 +41,23 @@ PFB_D typename RealOf<T>::type pivot_key(T x)
     return (m != m) ? (typename RealOf<T>::type)INFINITY : m;   // NaN is picked (and propagates)
 }
 
+// The column of the first maximum over the warp of (key >= 0, column): the
+// largest key, and among equal keys the smallest column.
+PFB_D unsigned first_max_col(double key, unsigned col)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(key);
+    const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)b;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    return __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? col : ~0u);
+}
+PFB_D unsigned first_max_col(float key, unsigned col)
+{
+    const unsigned b = (unsigned)__float_as_int(key);
+    const unsigned m = __reduce_max_sync(0xffffffffu, b);
+    return __reduce_min_sync(0xffffffffu, b == m ? col : ~0u);
+}
+
 template <typename T> PFB_D T phase_of(T a);
 template <> PFB_D float phase_of(float a) { return a < 0.f ? -1.f : 1.f; }
 template <> PFB_D double phase_of(double a) { return a < 0.0 ? -1.0 : 1.0; }
@@ -122,13 +139,22 @@ pf_small_kernel(const T *__restrict__ A, int64_t batch, int n, int flip,
 #pragma unroll 1
         for (int k = 0; k < n - 1; k += 2) {
             // ---- pivot: first maximum of |A[k][c]| over logical columns c > k
-            Real key = (lbl > k && lbl < n) ? pivot_key(R[0]) : (Real)(-1);
+            const bool cand = lbl > k && lbl < n;
+            Real key = cand ? pivot_key(R[0]) : (Real)(-1);
             int col = lbl;
+            if constexpr (G == 32) {
+                // one matrix per warp: warp reductions (redux.sync) on the key's
+                // bits -- a non-negative float compares as its bits -- then the
+                // smallest column among the equal keys; a lane without a
+                // candidate offers key 0 and column ~0, so it loses every tie
+                col = (int)first_max_col(cand ? key : (Real)0, cand ? (unsigned)lbl : ~0u);
+            } else {
 #pragma unroll
-            for (int off = G / 2; off > 0; off >>= 1) {
-                Real k2 = shfl_xor(key, off, G);
-                int c2 = shfl_xor(col, off, G);
-                if (k2 > key || (k2 == key && c2 < col)) { key = k2; col = c2; }
+                for (int off = G / 2; off > 0; off >>= 1) {
+                    Real k2 = shfl_xor(key, off, G);
+                    int c2 = shfl_xor(col, off, G);
+                    if (k2 > key || (k2 == key && c2 < col)) { key = k2; col = c2; }
+                }
             }
             const int j = col;
             const unsigned ball = __ballot_sync(0xffffffffu, lbl == j);
