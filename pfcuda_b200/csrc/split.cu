@@ -293,8 +293,11 @@ constexpr int kDeltaTileBytes = kSplitTileM * kDeltaLd * 8;   // 67,584
 // range of tiles, so consecutive tiles mostly share the A operand (the 128
 // trailing rows), which stays in shared memory.  The S digit-level accumulators
 // of a tile (NOUT * S * TN <= 448 TMEM columns) are handed back to the MMA
-// thread as soon as the epilogue has read them, so the next tile's MMAs overlap
-// this tile's FP64 read-modify-write.
+// thread once the epilogue has read them and, for real input, finished its
+// read-modify-write: the next tile's MMAs read their operands from shared
+// memory, and run alongside the read-modify-write both slowed down (a clock64
+// trace at 2n = 4096: 8.4k cycles a tile that way, 7.8k in turn).  The C store,
+// the next C load and the epilogue's waits still overlap the MMAs.
 //
 // Epilogue arithmetic: the tile value is 2^(e_a+e_b-56) * sum_l P_l 2^(7(6-l))
 // (fold_levels), added to C with one fused multiply-add.
@@ -326,6 +329,13 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
     // memory: an int8 MMA of 128 x 64 x 32 reading both operands from shared
     // memory (6 KB) is bound by its bandwidth, not by the tensor pipe.
     constexpr int kAcol0 = NOUT * S * TN;
+    // When the epilogue hands the accumulators back: real input (one output,
+    // 64-column MMAs) after its shared-memory read-modify-write, since the next
+    // tile's MMAs and that read-modify-write slow each other (update 21.6 ->
+    // 20.6 ms per call at 2n = 4096); complex input (two outputs, 32-column
+    // MMAs) right after reading them, where the overlap still pays (31.6
+    // against 32.6 ms at 2n = 2048).
+    constexpr bool kLateRelease = NOUT == 1;
     constexpr int kTmemA = (512 - kAcol0) / (KK / 4) < S ? (512 - kAcol0) / (KK / 4) : S;
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr int kk = KK;
@@ -515,8 +525,10 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
                     }
                 }
             }
-            tc_fence_before();
-            mbar_arrive(mb(5));
+            if constexpr (!kLateRelease) {
+                tc_fence_before();
+                mbar_arrive(mb(5));
+            }
             // this delta tile was last read by the reduce-adds of tile it - 2
             if (lane == 0 && it >= 2) bulk_wait_read1();
             epi_sync();
@@ -539,6 +551,10 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
                     }
                     *reinterpret_cast<double2 *>(db + r * kDeltaLd + d0 + 2 * pr) = v;
                 }
+            }
+            if constexpr (kLateRelease) {   // as in the round trip
+                tc_fence_before();
+                mbar_arrive(mb(5));
             }
             fence_proxy_async();
             epi_sync();
@@ -600,11 +616,19 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1, lim);
             ok = epi_all(w_ok);
             if (!ok) break;
+            if (kLateRelease && leader && it >= 1 && it + 1 < ntiles) {
+                // load tile it+1 into the buffer of tile it-1 (whose store,
+                // issued a phase ago, has read it by now) before the fold: its
+                // shared-memory writes then overlap the fold's TMEM reads and
+                // integer work instead of the read-modify-write below
+                bulk_wait_read0();
+                tl.step();
+                PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
+            }
             tc_fence_after();
             unsigned char *cb = sC + buf * kCTileBytes;
             // all of this thread's TMEM values first, folded to one double per
-            // output: the accumulators go back to the MMA thread before the
-            // shared-memory update, so the next tile's MMAs overlap it
+            // output (CW * NOUT registers)
             double dv[NOUT][CW];
 #pragma unroll
             for (int c8 = 0; c8 < CW / 8; c8++) {
@@ -625,35 +649,47 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
                     }
                 }
             }
-            tc_fence_before();
-            mbar_arrive(mb(5));
-            if (leader && it >= 1 && it + 1 < ntiles) {
-                // the store of tile it-1 has long read its buffer: load tile it+1 there
-                bulk_wait_read0();
-                tl.step();
-                PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
+            if constexpr (!kLateRelease) {
+                tc_fence_before();
+                mbar_arrive(mb(5));
+                if (leader && it >= 1 && it + 1 < ntiles) {
+                    // complex input: the next C tile is loaded here, after the
+                    // fold, where it was measured
+                    bulk_wait_read0();
+                    tl.step();
+                    PFB_LOAD_C(buf ^ 1, tl.I, tl.J);
+                }
             }
             // read-modify-write of the CW * NOUT doubles in shared memory:
-            // C += value * 2^(ea + eb - 56), one rounding
+            // C += value * 2^(ea + eb - 56), one rounding.  A chunk's loads are
+            // all issued before its stores, so their latencies overlap.
 #pragma unroll
             for (int c8 = 0; c8 < CW / 8; c8++) {
                 double sc[8];
 #pragma unroll
                 for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
                 const int d0 = h * 16 + c8 * 8 * NOUT;
+                double2 old[4 * NOUT];
+#pragma unroll
+                for (int pr = 0; pr < 4 * NOUT; pr++) old[pr] = *reinterpret_cast<const double2 *>(cb + cswz(r, d0 + 2 * pr));
 #pragma unroll
                 for (int pr = 0; pr < 4 * NOUT; pr++) {
-                    double2 *pp = reinterpret_cast<double2 *>(cb + cswz(r, d0 + 2 * pr));
-                    double2 old = *pp;
                     if (NOUT == 1) {
-                        old.x = fma(dv[0][c8 * 8 + 2 * pr], sc[2 * pr], old.x);
-                        old.y = fma(dv[0][c8 * 8 + 2 * pr + 1], sc[2 * pr + 1], old.y);
+                        old[pr].x = fma(dv[0][c8 * 8 + 2 * pr], sc[2 * pr], old[pr].x);
+                        old[pr].y = fma(dv[0][c8 * 8 + 2 * pr + 1], sc[2 * pr + 1], old[pr].y);
                     } else {
-                        old.x = fma(dv[0][c8 * 8 + pr], sc[pr], old.x);
-                        old.y = fma(dv[NOUT - 1][c8 * 8 + pr], sc[pr], old.y);
+                        old[pr].x = fma(dv[0][c8 * 8 + pr], sc[pr], old[pr].x);
+                        old[pr].y = fma(dv[NOUT - 1][c8 * 8 + pr], sc[pr], old[pr].y);
                     }
-                    *pp = old;
                 }
+#pragma unroll
+                for (int pr = 0; pr < 4 * NOUT; pr++) *reinterpret_cast<double2 *>(cb + cswz(r, d0 + 2 * pr)) = old[pr];
+            }
+            // real input: the accumulators go back to the MMA thread only now
+            // (kLateRelease)
+            if constexpr (kLateRelease) {
+                tc_fence_before();
+                mbar_arrive(mb(5));
             }
             // the tile in shared memory is complete: one thread stores it
             fence_proxy_async();

@@ -14,54 +14,54 @@ struct TuneEntry {
 };
 
 static const TuneEntry kTuneTable[] = {
-    {0, 1, 34, 544, 1LL, 1LL, 1, 7, 2, 1},  // n=512 batch=1: 1.033 ms
-    {0, 0, 34, 544, 1LL, 1LL, 1, 7, 2, 1},  // n=512 batch=1: 1.013 ms
-    {0, 1, 34, 544, 2LL, 221LL, 1, 7, 2, 1},  // n=512 batch=74: 1.238 ms
-    {0, 0, 34, 544, 2LL, 221LL, 1, 7, 2, 1},  // n=512 batch=74: 1.243 ms
-    {0, 1, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 1},  // n=512 batch=296: 2.590 ms
-    {0, 0, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 1},  // n=512 batch=296: 2.726 ms
-    {0, 1, 546, 1056, 1LL, 1LL, 1, 7, 2, 1},  // n=1024 batch=1: 2.101 ms
-    {0, 0, 546, 1056, 1LL, 1LL, 1, 7, 1, 1},  // n=1024 batch=1: 2.074 ms
-    {0, 1, 546, 1056, 2LL, 98LL, 1, 7, 1, 1},  // n=1024 batch=33: 2.729 ms
-    {0, 0, 546, 1056, 2LL, 98LL, 1, 7, 1, 1},  // n=1024 batch=33: 2.833 ms
-    {0, 1, 546, 1056, 99LL, 1099511627776LL, 2, 7, 1, 1},  // n=1024 batch=132: 5.967 ms
-    {0, 0, 546, 1056, 99LL, 1099511627776LL, 2, 7, 2, 1},  // n=1024 batch=132: 6.638 ms
-    {0, 1, 1058, 2080, 1LL, 1LL, 1, 7, 2, 1},  // n=2048 batch=1: 4.300 ms
-    {0, 0, 1058, 2080, 1LL, 1LL, 1, 7, 1, 1},  // n=2048 batch=1: 4.241 ms
-    {0, 1, 1058, 2080, 2LL, 44LL, 1, 7, 2, 1},  // n=2048 batch=15: 6.163 ms
-    {0, 0, 1058, 2080, 2LL, 44LL, 1, 7, 1, 1},  // n=2048 batch=15: 6.756 ms
-    {0, 1, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 1, 1},  // n=2048 batch=60: 15.238 ms
-    {0, 0, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 1, 1},  // n=2048 batch=60: 17.536 ms
-    {0, 1, 2082, 4160, 1LL, 1LL, 1, 7, 1, 1},  // n=4096 batch=1: 9.236 ms
-    {0, 0, 2082, 4160, 1LL, 1LL, 1, 7, 1, 1},  // n=4096 batch=1: 9.473 ms
-    {0, 1, 2082, 4160, 2LL, 20LL, 1, 7, 2, 1},  // n=4096 batch=7: 14.501 ms
-    {0, 0, 2082, 4160, 2LL, 20LL, 1, 7, 2, 1},  // n=4096 batch=7: 17.729 ms
-    {0, 1, 2082, 4160, 21LL, 1099511627776LL, 2, 7, 2, 1},  // n=4096 batch=22: 32.936 ms
-    {0, 0, 2082, 4160, 21LL, 1099511627776LL, 2, 7, 2, 1},  // n=4096 batch=22: 41.878 ms
-    {0, 1, 4162, 8224, 1LL, 1LL, 1, 7, 2, 1},  // n=6144 batch=1: 20.481 ms
-    {0, 0, 4162, 8224, 1LL, 1LL, 1, 7, 1, 1},  // n=6144 batch=1: 19.619 ms
-    {0, 1, 4162, 8224, 2LL, 20LL, 1, 7, 2, 1},  // n=6144 batch=7: 47.834 ms
-    {0, 0, 4162, 8224, 2LL, 20LL, 1, 7, 1, 1},  // n=6144 batch=7: 56.190 ms
-    {0, 1, 4162, 8224, 21LL, 1099511627776LL, 1, 7, 1, 1},  // n=6144 batch=9: 59.160 ms
-    {0, 0, 4162, 8224, 21LL, 1099511627776LL, 1, 7, 1, 1},  // n=6144 batch=9: 70.097 ms
-    {1, 1, 34, 544, 1LL, 1LL, 2, 7, 1, 1},  // n=512 batch=1: 1.522 ms
-    {1, 0, 34, 544, 1LL, 1LL, 2, 7, 2, 1},  // n=512 batch=1: 1.318 ms
-    {1, 1, 34, 544, 2LL, 221LL, 2, 7, 1, 1},  // n=512 batch=74: 2.221 ms
-    {1, 0, 34, 544, 2LL, 221LL, 2, 7, 1, 1},  // n=512 batch=74: 1.961 ms
-    {1, 1, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 1},  // n=512 batch=296: 5.547 ms
-    {1, 0, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 1},  // n=512 batch=296: 4.763 ms
-    {1, 1, 546, 1056, 1LL, 1LL, 2, 7, 2, 1},  // n=1024 batch=1: 3.129 ms
-    {1, 0, 546, 1056, 1LL, 1LL, 2, 7, 1, 1},  // n=1024 batch=1: 2.699 ms
-    {1, 1, 546, 1056, 2LL, 98LL, 2, 7, 1, 1},  // n=1024 batch=33: 5.384 ms
-    {1, 0, 546, 1056, 2LL, 98LL, 2, 7, 1, 1},  // n=1024 batch=33: 4.819 ms
-    {1, 1, 546, 1056, 99LL, 1099511627776LL, 2, 7, 2, 1},  // n=1024 batch=132: 14.233 ms
-    {1, 0, 546, 1056, 99LL, 1099511627776LL, 2, 7, 2, 1},  // n=1024 batch=132: 12.683 ms
-    {1, 1, 1058, 2080, 1LL, 1LL, 2, 7, 2, 1},  // n=2048 batch=1: 6.554 ms
-    {1, 0, 1058, 2080, 1LL, 1LL, 2, 7, 1, 1},  // n=2048 batch=1: 5.833 ms
-    {1, 1, 1058, 2080, 2LL, 44LL, 2, 7, 2, 1},  // n=2048 batch=15: 13.602 ms
-    {1, 0, 1058, 2080, 2LL, 44LL, 2, 7, 2, 1},  // n=2048 batch=15: 12.804 ms
-    {1, 1, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 2, 1},  // n=2048 batch=44: 29.985 ms
-    {1, 0, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 2, 1},  // n=2048 batch=44: 28.418 ms
+    {0, 1, 34, 544, 1LL, 1LL, 1, 7, 2, 1},  // n=512 batch=1: 1.044 ms
+    {0, 0, 34, 544, 1LL, 1LL, 1, 7, 2, 1},  // n=512 batch=1: 1.028 ms
+    {0, 1, 34, 544, 2LL, 221LL, 1, 7, 2, 2},  // n=512 batch=74: 1.228 ms
+    {0, 0, 34, 544, 2LL, 221LL, 1, 7, 1, 1},  // n=512 batch=74: 1.243 ms
+    {0, 1, 34, 544, 222LL, 1099511627776LL, 2, 7, 1, 2},  // n=512 batch=296: 2.537 ms
+    {0, 0, 34, 544, 222LL, 1099511627776LL, 2, 7, 1, 1},  // n=512 batch=296: 2.728 ms
+    {0, 1, 546, 1056, 1LL, 1LL, 1, 7, 2, 1},  // n=1024 batch=1: 2.130 ms
+    {0, 0, 546, 1056, 1LL, 1LL, 1, 7, 1, 1},  // n=1024 batch=1: 2.101 ms
+    {0, 1, 546, 1056, 2LL, 98LL, 1, 7, 2, 2},  // n=1024 batch=33: 2.667 ms
+    {0, 0, 546, 1056, 2LL, 98LL, 1, 7, 1, 1},  // n=1024 batch=33: 2.831 ms
+    {0, 1, 546, 1056, 99LL, 1099511627776LL, 2, 7, 2, 2},  // n=1024 batch=132: 5.783 ms
+    {0, 0, 546, 1056, 99LL, 1099511627776LL, 2, 7, 1, 1},  // n=1024 batch=132: 6.639 ms
+    {0, 1, 1058, 2080, 1LL, 1LL, 1, 7, 2, 1},  // n=2048 batch=1: 4.333 ms
+    {0, 0, 1058, 2080, 1LL, 1LL, 1, 7, 1, 1},  // n=2048 batch=1: 4.253 ms
+    {0, 1, 1058, 2080, 2LL, 44LL, 1, 7, 2, 2},  // n=2048 batch=15: 5.947 ms
+    {0, 0, 1058, 2080, 2LL, 44LL, 1, 7, 2, 1},  // n=2048 batch=15: 6.751 ms
+    {0, 1, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 1, 2},  // n=2048 batch=60: 14.519 ms
+    {0, 0, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 2, 1},  // n=2048 batch=60: 17.550 ms
+    {0, 1, 2082, 4160, 1LL, 1LL, 1, 7, 2, 1},  // n=4096 batch=1: 9.256 ms
+    {0, 0, 2082, 4160, 1LL, 1LL, 1, 7, 1, 1},  // n=4096 batch=1: 9.453 ms
+    {0, 1, 2082, 4160, 2LL, 20LL, 1, 7, 1, 2},  // n=4096 batch=7: 13.873 ms
+    {0, 0, 2082, 4160, 2LL, 20LL, 1, 7, 2, 1},  // n=4096 batch=7: 17.717 ms
+    {0, 1, 2082, 4160, 21LL, 1099511627776LL, 2, 7, 2, 2},  // n=4096 batch=28: 34.758 ms
+    {0, 0, 2082, 4160, 21LL, 1099511627776LL, 2, 7, 1, 1},  // n=4096 batch=28: 50.672 ms
+    {0, 1, 4162, 8224, 1LL, 1LL, 1, 7, 1, 2},  // n=6144 batch=1: 20.188 ms
+    {0, 0, 4162, 8224, 1LL, 1LL, 1, 7, 1, 1},  // n=6144 batch=1: 19.664 ms
+    {0, 1, 4162, 8224, 2LL, 20LL, 1, 7, 2, 1},  // n=6144 batch=7: 44.561 ms
+    {0, 0, 4162, 8224, 2LL, 20LL, 1, 7, 1, 1},  // n=6144 batch=7: 56.813 ms
+    {0, 1, 4162, 8224, 21LL, 1099511627776LL, 1, 7, 1, 1},  // n=6144 batch=13: 72.602 ms
+    {0, 0, 4162, 8224, 21LL, 1099511627776LL, 1, 7, 1, 1},  // n=6144 batch=13: 98.274 ms
+    {1, 1, 34, 544, 1LL, 1LL, 2, 7, 1, 1},  // n=512 batch=1: 1.547 ms
+    {1, 0, 34, 544, 1LL, 1LL, 2, 7, 2, 1},  // n=512 batch=1: 1.336 ms
+    {1, 1, 34, 544, 2LL, 221LL, 2, 7, 1, 2},  // n=512 batch=74: 2.144 ms
+    {1, 0, 34, 544, 2LL, 221LL, 2, 7, 2, 1},  // n=512 batch=74: 1.963 ms
+    {1, 1, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 2},  // n=512 batch=296: 5.421 ms
+    {1, 0, 34, 544, 222LL, 1099511627776LL, 2, 7, 2, 1},  // n=512 batch=296: 4.764 ms
+    {1, 1, 546, 1056, 1LL, 1LL, 2, 7, 2, 1},  // n=1024 batch=1: 3.154 ms
+    {1, 0, 546, 1056, 1LL, 1LL, 2, 7, 1, 1},  // n=1024 batch=1: 2.718 ms
+    {1, 1, 546, 1056, 2LL, 98LL, 2, 7, 2, 2},  // n=1024 batch=33: 5.171 ms
+    {1, 0, 546, 1056, 2LL, 98LL, 2, 7, 2, 1},  // n=1024 batch=33: 4.813 ms
+    {1, 1, 546, 1056, 99LL, 1099511627776LL, 2, 7, 1, 1},  // n=1024 batch=132: 13.993 ms
+    {1, 0, 546, 1056, 99LL, 1099511627776LL, 2, 7, 1, 1},  // n=1024 batch=132: 12.681 ms
+    {1, 1, 1058, 2080, 1LL, 1LL, 2, 7, 2, 1},  // n=2048 batch=1: 6.551 ms
+    {1, 0, 1058, 2080, 1LL, 1LL, 2, 7, 2, 1},  // n=2048 batch=1: 5.858 ms
+    {1, 1, 1058, 2080, 2LL, 44LL, 2, 7, 2, 2},  // n=2048 batch=15: 13.028 ms
+    {1, 0, 1058, 2080, 2LL, 44LL, 2, 7, 2, 1},  // n=2048 batch=15: 12.805 ms
+    {1, 1, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 1, 1},  // n=2048 batch=59: 40.786 ms
+    {1, 0, 1058, 2080, 45LL, 1099511627776LL, 2, 7, 1, 1},  // n=2048 batch=59: 36.973 ms
 };
 
 // The first entry for this dtype class and mode whose order and batch bins
