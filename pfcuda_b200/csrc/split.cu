@@ -31,6 +31,7 @@
 // Every mbarrier wait is bounded; a wait that gives up marks the matrix in
 // SplitArgs::err and the kernel frees its TMEM and returns.
 #include <cuda.h>
+#include <limits.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -233,6 +234,20 @@ PFB_D double exp2i(int e)
 {
     if (e >= -1022 && e <= 1023) return __longlong_as_double((long long)(e + 1023) << 52);
     return scalbn(1.0, e);
+}
+
+// The tile scale 2^(ea + eb - 56): from its exponent bits when the warp's
+// scales are all in the normal range (fast, decided by one vote), else exp2i.
+PFB_D bool scales_normal(int ea, int eb, bool has_eb)
+{
+    const int a0 = __reduce_min_sync(0xffffffffu, ea), a1 = __reduce_max_sync(0xffffffffu, ea);
+    const int b0 = __reduce_min_sync(0xffffffffu, has_eb ? eb : INT_MAX);
+    const int b1 = __reduce_max_sync(0xffffffffu, has_eb ? eb : INT_MIN);
+    return a0 + b0 - 56 >= -1022 && a1 + b1 - 56 <= 1023;
+}
+PFB_D double scale2(int ea, int eb, bool fast)
+{
+    return fast ? __hiloint2double((ea + eb - 56 + 1023) << 20, 0) : exp2i(ea + eb - 56);
 }
 
 // An integer |v| < 2^51 as a double, exactly, by the usual magic-number
@@ -502,6 +517,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             const int bc0 = k1 + tw.J * TN + h * CW;
             const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
             const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
+            // every scale of this warp's block (its rows' ea against its
+            // columns' eb) is a normal power of two
+            const bool fast = scales_normal(ea, eb_l, lane < CW);
             ok = epi_all(mbar_wait_bounded(mb(4), it & 1, lim));
             if (!ok) break;
             tc_fence_after();
@@ -537,7 +555,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             for (int c8 = 0; c8 < CW / 8; c8++) {
                 double sc[8];
 #pragma unroll
-                for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
+                for (int c = 0; c < 8; c++) sc[c] = scale2(ea, __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c), fast);
                 const int d0 = h * 16 + c8 * 8 * NOUT;
 #pragma unroll
                 for (int pr = 0; pr < 4 * NOUT; pr++) {
@@ -611,6 +629,9 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             const int bc0 = k1 + tw.J * TN + h * CW;
             const int ea = arow < n ? __ldg(&sa.ex[b * n + arow]) : 0;
             const int eb_l = (lane < CW && bc0 + lane < n) ? __ldg(&sa.ex[b * n + bc0 + lane]) : 0;
+            // every scale of this warp's block (its rows' ea against its
+            // columns' eb) is a normal power of two
+            const bool fast = scales_normal(ea, eb_l, lane < CW);
             bool w_ok = mbar_wait_bounded(mb(6 + buf), (it >> 1) & 1, lim);
             if (w_ok) c_done = it + 1;
             if (w_ok) w_ok = mbar_wait_bounded(mb(4), it & 1, lim);
@@ -667,7 +688,7 @@ split_update_kernel(const __grid_constant__ CUtensorMap cmap, double *__restrict
             for (int c8 = 0; c8 < CW / 8; c8++) {
                 double sc[8];
 #pragma unroll
-                for (int c = 0; c < 8; c++) sc[c] = exp2i(ea + __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c) - 56);
+                for (int c = 0; c < 8; c++) sc[c] = scale2(ea, __shfl_sync(0xffffffffu, eb_l, c8 * 8 + c), fast);
                 const int d0 = h * 16 + c8 * 8 * NOUT;
                 double2 old[4 * NOUT];
 #pragma unroll
