@@ -504,10 +504,12 @@ def _hbm_peak_source():
         return "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
-# DRAM read+write bytes over algorithmic bytes per launch for kernels captured
-# with ncu after the first captures quoted at the roofline block below
-# (filled from the profiles of this engine's later kernels; None: not captured)
-TRAFFIC_RATIO_MEASURED = {}
+# DRAM read+write bytes over algorithmic bytes per launch for kernel variants
+# captured with ncu after the first captures quoted at the roofline block
+# below: the reduce-add split epilogue at k0 = 640 of 2n = 4096, batch 2
+# (145.6 MB against 184.1 MB), the configuration the table picks for the
+# headline
+TRAFFIC_RATIO_MEASURED = {"split_update_kernel_reduce": 0.79}
 
 
 def auto_batch(n, dtype="float64"):
@@ -789,7 +791,7 @@ def main():
                 "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": tr * panel_bytes / npan if tr else None,
                 "note": "latency-bound: 32 dependent pivot steps per launch, each a cluster barrier and a "
-                        "global load of the interchanged row (~7k cycles per step); algorithmic bytes = "
+                        "global load of the interchanged row (8-11k cycles per step); algorithmic bytes = "
                         "panel rows read and written once; traffic per launch scaled from ncu"}
     else:
         kname = "split_update_kernel" if head == "split" else "gemm_dmma_kernel"
