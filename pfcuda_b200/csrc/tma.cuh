@@ -1,5 +1,5 @@
 // tma.cuh -- mbarriers, bulk tensor (TMA) loads and the tensor-map encoder
-// shared by the split update (split.cu) and the panel (panel.cuh).
+// of the split update (split.cu).
 #pragma once
 
 #include <cuda.h>
@@ -46,9 +46,6 @@ PFB_D void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z
                  " [%0], [%1, {%2, %3, %4}], [%5];"
                  ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
 }
-// orders this thread's earlier generic-proxy global writes before later
-// async-proxy (TMA) reads of the same addresses
-PFB_D void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
