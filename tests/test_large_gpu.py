@@ -322,3 +322,28 @@ def test_split_timeout_path_marks_only_its_matrix():
     la2, sg2 = pf.slog_pfaffian_raw(X, mode="split")
     assert np.all(np.abs(la2.cpu().numpy() - wl) <= 1e-10 * np.abs(wl))
     assert np.array_equal(sg2.cpu().numpy(), wsg)
+
+
+@pytest.mark.parametrize("mode,epilogue", [("fp64", None), ("split", "roundtrip"), ("split", "reduce"),
+                                           ("split", "direct")])
+@pytest.mark.parametrize("n", [130, 514])
+def test_extreme_scales_match_the_exact_relation(mode, epilogue, n):
+    """Pf(D A D) = det(D) Pf(A) for a diagonal D, so with D of powers of two
+    log|Pf(DAD)| = sum log d_i + log|Pf(A)| and the sign is Pf(A)'s.  Every
+    other index scaled by 2^-490: the split update's increments between two
+    scaled indices need the scale 2^(e_a + e_b - 56) ~ 2^-1036, below the
+    normal range, which the epilogue forms by the general path instead of
+    from exponent bits; all matrix entries stay normal (~2^-980 and up)."""
+    rng = np.random.default_rng(1200 + n)
+    A = O.skew_normal(rng, 2, n, scale=1 / np.sqrt(n))
+    d = np.where(np.arange(n) % 2 == 0, 2.0 ** -490, 1.0)
+    As = A * d[None, :, None] * d[None, None, :]
+    cfg = None if epilogue is None else {"epilogue": epilogue}
+    la, sg = pf.slog_pfaffian_raw(cuda(As), mode=mode, config=cfg)
+    la, sg = la.cpu().numpy(), sg.cpu().numpy()
+    wl, ws = O.slog_pf(A)
+    shift = float(np.sum(np.log(d)))
+    # 1e-8 absolute: la sums ~n/2 logs of about -340 each (their rounding); a
+    # lost or wrong scale would move log|Pf| by O(1)
+    assert np.all(np.abs((la - shift) - wl) <= 1e-10 * np.abs(wl) + 1e-8), np.abs((la - shift) - wl).max()
+    assert np.array_equal(sg, ws)
